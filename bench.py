@@ -1,0 +1,361 @@
+"""Benchmark: SSP-RK3 cell-updates/s of the 3-D Kelvin-Helmholtz set-up.
+
+Workload (one "step" = one SSP-RK3 step = 3 fused stage passes): periodic
+unit cube of 256^3 interior cells, float32, WENO5-JS + HLLC + viscous
+(nu = 1e-4, Pr = 0.7), CFL 0.5 with the time step reduced on the device.
+Seeded synthetic initial condition (swirlc_b200.configs.kelvin_helmholtz).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank advances its own 256^3 domain (weak scaling,
+replicas; the halo exchange of a decomposed domain is a separate path).
+`value` is the whole-job cell-updates/s (all ranks' cells x K / max time).
+`e2e` times the public API call `Simulation.step` with the state copied from
+pinned host memory and the result copied back every step.
+`--impl reference` times the CPU oracle (the NumPy restatement of the
+reference path) on this host's cores over a bounded sample of the same
+workload; the reference's own TensorFlow path cannot run here.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+  sys.path.insert(0, ROOT)
+
+N_CELLS_EDGE = 256
+ALG_BYTES_PER_CELL_UPDATE = 160  # fp32: 40 + 60 + 60 B over the 3 stages
+METRIC = 'RK3 cell-updates/s at 256^3 fp32 (% HBM roofline)'
+UNIT = 'cell-updates/s'
+
+
+def _env_rank():
+  return (int(os.environ.get('RANK', '0')), int(os.environ.get('WORLD_SIZE', '1')),
+          int(os.environ.get('LOCAL_RANK', '0')))
+
+
+def _peaks():
+  path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+  try:
+    with open(path) as f:
+      p = json.load(f)
+    return float(p['hbm_gbs']), 'measured'
+  except (OSError, KeyError, ValueError):
+    return 6650.0, 'fallback'
+
+
+def _traffic_from_profiles():
+  """Per-launch DRAM bytes of the stage kernel from the committed ncu summary."""
+  path = os.path.join(ROOT, 'profiles', 'stage_kernel_kh.txt')
+  try:
+    with open(path) as f:
+      for line in f:
+        if line.startswith('traffic_bytes_per_cell_stage:'):
+          return float(line.split(':', 1)[1])
+  except OSError:
+    pass
+  return None
+
+
+class ClockSampler:
+  """Samples nvidia-smi clocks/throttle reasons in the background."""
+
+  Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+       'clocks_event_reasons.hw_slowdown,'
+       'clocks_event_reasons.hw_thermal_slowdown,'
+       'clocks_event_reasons.sw_thermal_slowdown,'
+       'clocks_event_reasons.sw_power_cap')
+
+  def __init__(self, index: int):
+    self.index = index
+    self.proc = None
+    self.path = None
+
+  def start(self):
+    fd, self.path = tempfile.mkstemp(suffix='.csv')
+    os.close(fd)
+    try:
+      self.proc = subprocess.Popen(
+          ['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.Q}',
+           '--format=csv,noheader,nounits', '-lms', '200'],
+          stdout=open(self.path, 'w'), stderr=subprocess.DEVNULL)
+    except OSError:
+      self.proc = None
+
+  def stop(self):
+    if self.proc is None:
+      return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unavailable']}
+    self.proc.terminate()
+    try:
+      self.proc.wait(timeout=5)
+    except subprocess.TimeoutExpired:
+      self.proc.kill()
+    sm, smax, reasons = [], [], set()
+    names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+             'sw_power_cap']
+    with open(self.path) as f:
+      for line in f:
+        parts = [p.strip() for p in line.split(',')]
+        if len(parts) < 9:
+          continue
+        try:
+          sm.append(float(parts[1]))
+          smax.append(float(parts[2]))
+        except ValueError:
+          continue
+        for name, val in zip(names, parts[5:9]):
+          if val.lower() in ('active', '0x1') or val.startswith('Active'):
+            reasons.add(name)
+    os.unlink(self.path)
+    return {'sm_mhz': statistics.median(sm) if sm else None,
+            'sm_max_mhz': max(smax) if smax else None,
+            'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def run_ours(args):
+  import torch
+  import torch.distributed as dist
+  from swirlc_b200 import _native as nat
+  from swirlc_b200 import configs, engine
+  from swirlc_b200.core import parameter, simulation
+  from swirlc_b200.physics import physics_models
+
+  rank, world, local = _env_rank()
+  torch.cuda.set_device(local)
+  if world > 1:
+    dist.init_process_group('nccl', timeout=__import__('datetime').timedelta(seconds=120))
+  n = args.n
+  user_cfg, state = configs.kelvin_helmholtz(n=n, seed=rank)
+  cfg = parameter.SwirlCParameters(user_cfg)
+  pm = physics_models.PhysicsModels(cfg)
+  dev = torch.device('cuda', local)
+  fields = [torch.tensor(state[k], device=dev) for k in
+            ('rho', 'rho_u', 'rho_v', 'rho_w', 'rho_e')]
+  solver = engine.Solver(cfg, pm, fields[0].shape, torch.float32, dev)
+  stepper = engine.Stepper(solver, fields, dt=cfg.dt, cfl=cfg.cfl)
+  # Warm-up (eager), then capture one step and warm the graph.
+  stepper.step(1)
+  torch.cuda.synchronize()
+  c0 = nat.launch_count()
+  stepper.capture()
+  launches_per_step = nat.launch_count() - c0
+  stepper.step(max(args.warmup - 1, 1))
+  torch.cuda.synchronize()
+  cells = n ** 3
+
+  def barrier():
+    if world > 1:
+      dist.barrier()
+
+  sampler = ClockSampler(local)
+  sampler.start()
+  barrier()
+  torch.cuda.synchronize()
+  ev0 = torch.cuda.Event(enable_timing=True)
+  ev1 = torch.cuda.Event(enable_timing=True)
+  ev0.record()
+  stepper.step(args.steps)
+  ev1.record()
+  torch.cuda.synchronize()
+  barrier()
+  clocks = sampler.stop()
+  ms = ev0.elapsed_time(ev1)
+  if world > 1:
+    t = torch.tensor([ms], device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+  value = world * cells * args.steps / (ms / 1e3)
+
+  # Stage-kernel durations (eager launches bracketed by events on the
+  # launching stream), for the roofline of the dominant kernel.
+  nstage_steps = 3
+  s = solver
+  dt = stepper.clock[1:2]
+  evs = []
+  for _ in range(nstage_steps):
+    s.fill_halos(stepper.u)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(); s.stage(stepper.u, None, stepper.w1, nat.SWC_OUT_EULER, dt=dt); b.record()
+    evs.append((a, b, 40))
+    s.fill_halos(stepper.w1)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(); s.stage(stepper.w1, stepper.u, stepper.w2, nat.SWC_OUT_CONVEX, 0.75, 0.25, dt=dt); b.record()
+    evs.append((a, b, 60))
+    s.fill_halos(stepper.w2)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(); s.stage(stepper.w2, stepper.u, stepper.u, nat.SWC_OUT_CONVEX, 1 / 3, 2 / 3, dt=dt); b.record()
+    evs.append((a, b, 60))
+  torch.cuda.synchronize()
+  tot_bytes = sum(bpc * cells for _, _, bpc in evs)
+  tot_ms = sum(a.elapsed_time(b) for a, b, _ in evs)
+  achieved = tot_bytes / (tot_ms / 1e3) / 1e9
+  peak, peak_kind = _peaks()
+  traffic_pc = _traffic_from_profiles()
+
+  # End-to-end through the public API: host state -> Simulation.step -> host.
+  sim = simulation.Simulation(None, cfg)
+  names = ('rho', 'rho_u', 'rho_v', 'rho_w', 'rho_e')
+  host = {k: torch.from_numpy(state[k]).pin_memory() for k in names}
+  host_out = {k: torch.empty_like(host[k]).pin_memory() for k in names}
+  replicas = np.array([[[0]]])
+  e2e_steps = max(1, min(args.steps, 5))
+
+  def e2e_once():
+    dev_state = {k: host[k].to(dev, non_blocking=True) for k in names}
+    out = sim.step(0, replicas, 0, dev_state, {})
+    for k in names:
+      host_out[k].copy_(out[k], non_blocking=True)
+
+  e2e_once()
+  torch.cuda.synchronize()
+  barrier()
+  t0 = time.perf_counter()
+  ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+  ea.record()
+  for _ in range(e2e_steps):
+    e2e_once()
+  eb.record()
+  torch.cuda.synchronize()
+  e2e_ms = ea.elapsed_time(eb)
+  if world > 1:
+    t = torch.tensor([e2e_ms], device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+  state_bytes = sum(host[k].numel() * 4 for k in names)
+
+  cpu = None
+  if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    cpu = cpu_baseline_sample(args.cpu_sample)
+
+  if rank == 0:
+    line = {
+        'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world,
+        'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': ms / args.steps, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+        'data': 'synthetic (seeded KH initial condition, configs.kelvin_helmholtz)',
+        'config': {'workload': f'kelvin_helmholtz {n}^3 fp32 WENO5+HLLC+viscous, '
+                               'SSP-RK3, CFL 0.5, device dt',
+                   'cells_per_gpu': cells, 'halo_width': 3,
+                   'parallelism': f'replicas x{world}',
+                   'l2_flush': 'inputs larger than L2 (5 fields x 262^3 x 4 B '
+                               '= 360 MB per state)',
+                   'graph': 'one RK3 step captured in a CUDA graph'},
+        'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak,
+                     'unit': 'GB/s', 'frac': achieved / peak,
+                     'peak_source': peak_kind,
+                     'traffic': None if traffic_pc is None else traffic_pc * cells,
+                     'kernel': 'stage_kernel (3 launches per step, algorithmic '
+                               '40/60/60 B per cell)'},
+        'cpu_baseline': cpu,
+        'e2e': {'value': world * cells * e2e_steps / (e2e_ms / 1e3), 'unit': UNIT,
+                'h2d_bytes_per_step': state_bytes,
+                'd2h_bytes_per_step': state_bytes,
+                'api': 'swirlc_b200.core.simulation.Simulation.step'},
+        'gpu_launches': launches_per_step * args.steps,
+        'clocks': clocks,
+    }
+    print(json.dumps(line), flush=True)
+  del stepper.graph
+  if world > 1:
+    dist.destroy_process_group()
+
+
+def _oracle_rk3_worker(payload):
+  import numpy as _np
+  from oracle import swirlc_oracle as orc
+  cfg, state = payload
+  t0 = time.perf_counter()
+  orc.rk3(state, cfg.dt, lambda s: orc.rhs(s, cfg))
+  return time.perf_counter() - t0
+
+
+def cpu_baseline_sample(n_sample: int, procs: int = 1):
+  """Times the CPU oracle (NumPy float32) on one RK3 step of the KH set-up
+  at n_sample^3, `procs` independent samples in parallel processes."""
+  import multiprocessing as mp
+  from swirlc_b200 import configs
+  from oracle import swirlc_oracle as orc
+  user_cfg, state = configs.kelvin_helmholtz(n=n_sample)
+  keys = ('halo_width', 'dx', 'dy', 'dz', 'interpolation_scheme',
+          'numeric_flux_scheme', 'include_diffusion', 'transport_parameters',
+          'x', 'y', 'z', 'bc', 'dt')
+  ocfg = orc.make_cfg(**{k: user_cfg[k] for k in keys if k in user_cfg})
+  ocfg.bc = orc.periodic_bc()
+  if procs <= 1:
+    secs = _oracle_rk3_worker((ocfg, state))
+    total = n_sample ** 3 / secs
+  else:
+    ctx = mp.get_context('spawn')
+    with ctx.Pool(procs) as pool:
+      t0 = time.perf_counter()
+      pool.map(_oracle_rk3_worker, [(ocfg, state)] * procs)
+      secs = time.perf_counter() - t0
+    total = procs * n_sample ** 3 / secs
+  return {'value': total, 'unit': UNIT, 'cores': procs, 'kind': 'port',
+          'sample': f'one SSP-RK3 step of KH at {n_sample}^3 (WENO5+HLLC+'
+                    f'viscous) per process, NumPy float32 oracle, '
+                    f'{secs:.1f} s wall'}
+
+
+def run_reference(args):
+  rank, world, _ = _env_rank()
+  if rank != 0:
+    return
+  procs = os.cpu_count() or 1
+  vals = []
+  for _ in range(max(1, min(args.steps, 5))):
+    vals.append(cpu_baseline_sample(args.cpu_sample, procs))
+  v = statistics.median(x['value'] for x in vals)
+  base = vals[0]
+  line = {
+      'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': UNIT,
+      'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+      'ms_per_step': args.n ** 3 / v * 1e3, 'higher_is_better': True,
+      'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+      'data': 'synthetic (seeded KH initial condition)',
+      'config': {'workload': f'kelvin_helmholtz {args.n}^3 fp32 WENO5+HLLC+'
+                             'viscous, SSP-RK3 (CPU sample '
+                             f'{args.cpu_sample}^3 per process)',
+                 'parallelism': f'{procs} host processes'},
+      'cpu_baseline': {'value': v, 'unit': UNIT, 'cores': procs,
+                       'kind': 'port', 'sample': base['sample']},
+      'e2e': {'value': v, 'unit': UNIT, 'h2d_bytes_per_step': 0,
+              'd2h_bytes_per_step': 0},
+      'note': 'the reference TensorFlow path needs TensorFlow and swirl_lm, '
+              'which are not installed; the NumPy oracle restating it runs',
+  }
+  print(json.dumps(line), flush=True)
+
+
+def main():
+  ap = argparse.ArgumentParser()
+  ap.add_argument('--gpus', type=int, default=1)
+  ap.add_argument('--steps', type=int, default=20)
+  ap.add_argument('--warmup', type=int, default=3)
+  ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+  ap.add_argument('--n', type=int, default=N_CELLS_EDGE)
+  ap.add_argument('--cpu-sample', type=int, default=96)
+  ap.add_argument('--no-cpu-baseline', action='store_true')
+  args = ap.parse_args()
+  if args.warmup < 3:
+    args.warmup = 3
+  if args.impl == 'reference':
+    run_reference(args)
+  else:
+    run_ours(args)
+
+
+if __name__ == '__main__':
+  main()

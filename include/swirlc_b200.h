@@ -1,0 +1,203 @@
+/*
+ * swirlc_b200 C-ABI: B200 (sm_100a) kernels for Swirl-C's compressible
+ * finite-volume right-hand side, its halo fill, the SSP-RK3/RK2 stage update
+ * and the CFL time-step reduction.
+ *
+ * Conventions shared by every entry point
+ *  - Fields are device arrays in the reference layout [nz+2h][nx+2h][ny+2h]
+ *    (y fastest), halos included; `SwcGrid.sx` / `.sz` give the element
+ *    strides of x and z (the y stride is 1).
+ *  - Conserved fields come in the order rho, rho_u, rho_v, rho_w, rho_e,
+ *    followed by `SwcScheme.nscalars` transported scalars rho_phi.
+ *  - A face value stored at index i belongs to face i-1/2, as in the
+ *    reference (compressible_navier_stokes.py:442-453).
+ *  - `stream` is a cudaStream_t passed as void*; every call is asynchronous
+ *    on that stream and allocates nothing.
+ *  - Every call returns SWC_OK (0) or a negative status; swc_last_error()
+ *    gives the message of the last failing call on the calling thread. No
+ *    C++ exception crosses this boundary.
+ */
+#ifndef SWIRLC_B200_H_
+#define SWIRLC_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWC_ABI_VERSION 1
+#define SWC_MAX_FIELDS 8 /* 5 conserved + up to 3 transported scalars */
+
+/* Status codes. */
+enum {
+  SWC_OK = 0,
+  SWC_ERR_ARG = -1,         /* bad pointer, size or enum (ValueError)      */
+  SWC_ERR_UNSUPPORTED = -2, /* configuration not implemented (NotImplementedError) */
+  SWC_ERR_LAUNCH = -3,      /* CUDA launch or runtime failure              */
+  SWC_ERR_TIMEOUT = -4,     /* a bounded device wait gave up               */
+  SWC_ERR_NONFINITE = -5    /* non-finite value detected                   */
+};
+
+enum { SWC_F32 = 0, SWC_F64 = 1 };
+/* interpolation_scheme (compressible_navier_stokes.py:39-43); SWC_NODE is
+ * the identity face value used by the reference tests' WENO mock. */
+enum { SWC_WENO5 = 0, SWC_WENO3 = 1, SWC_MUSCL = 2, SWC_NODE = 3 };
+enum { SWC_LIM_VAN_LEER = 0, SWC_LIM_MC = 1, SWC_LIM_MINMOD = 2 };
+/* numeric_flux_scheme (riemann_solver.py:24-27). */
+enum { SWC_HLL = 0, SWC_HLLC = 1 };
+/* BoundaryCondition (bc_types.py:22-27) plus NONE = leave the halo as is. */
+enum { SWC_BC_PERIODIC = 0, SWC_BC_DIRICHLET = 1, SWC_BC_NEUMANN = 2,
+       SWC_BC_NONE = 4 };
+/* Stage output modes: RHS: out = L(uk); EULER: out = uk + L*dt;
+ * CONVEX: out = u0*c0 + (uk + L*dt)*c1 (rk3.py:69-83);
+ * AVERAGE: out = c0*(u0 + (uk + dt*L)) (rk2.py:67-86). */
+enum { SWC_OUT_RHS = 0, SWC_OUT_EULER = 1, SWC_OUT_CONVEX = 2,
+       SWC_OUT_AVERAGE = 3 };
+
+typedef struct SwcGrid {
+  int32_t nx, ny, nz; /* interior cells along x, y, z                    */
+  int32_t halo;       /* halo layers stored on each side (cfg.halo_width) */
+  int64_t sx, sz;     /* element strides of x and z                      */
+  double dx, dy, dz;  /* cfg.dx, cfg.dy, cfg.dz                          */
+} SwcGrid;
+
+typedef struct SwcScheme {
+  int32_t dtype;     /* SWC_F32 / SWC_F64                                   */
+  int32_t interp;    /* SWC_WENO5 ...                                       */
+  int32_t limiter;   /* MUSCL limiter, SWC_LIM_*                             */
+  int32_t riemann;   /* SWC_HLL / SWC_HLLC                                   */
+  int32_t diffusion; /* cfg.include_diffusion                               */
+  int32_t nscalars;  /* transported scalars after rho_e (0..3)              */
+  int32_t gravity_mask; /* bit d set: rho_u_d gets rho*G*g[d] (gravity.py:51-102) */
+  int32_t zseg;      /* z planes per CTA in the stage kernel; 0 = automatic */
+  int32_t tile;      /* stage tile shape: 0 = 32x8 (y x x), 1 = 16x16, 2 = 8x32 */
+  int32_t reserved;
+  double nu, pr;     /* transport_parameters (simple.py:44-45)              */
+  double g[3];       /* cfg.g, the gravity unit vector                      */
+  /* Per-axis gravitational terms a_d[i] = G*g_d*coord_d[i] on the local
+   * cell-centre mesh with halos (generic.py:282-319, utils.py:43-89); the
+   * potential energy is (-a_x - a_y) - a_z. NULL means zero. Arrays are in
+   * `dtype` with n_d + 2*halo entries. */
+  const void* pe_axis[3];
+} SwcScheme;
+
+typedef struct SwcBC {
+  int32_t kind;      /* SWC_BC_*                                            */
+  int32_t per_layer; /* 0: `value` in every layer; 1: `planes` per layer    */
+  double value;      /* Dirichlet value or Neumann increment per layer      */
+  /* Dirichlet planes [halo][A][B] in `dtype`; (A, B) are the two other axes
+   * in storage order (z, x, y) with halos: x-faces (z, y), y-faces (z, x),
+   * z-faces (x, y). Layer 0 is the outermost layer on the low side and the
+   * innermost on the high side (boundary_test.py:175-298). */
+  const void* planes;
+} SwcBC;
+
+typedef struct SwcFieldBC {
+  int32_t via_primitive; /* BC given on field/rho (boundary.py:516-531)     */
+  int32_t reserved;
+  SwcBC side[3][2];      /* [x, y, z][low, high]                            */
+} SwcFieldBC;
+
+/* Device-resident time control used by the step loop without host syncs. */
+typedef struct SwcClock {
+  double t;       /* simulated time                                      */
+  double dt;      /* step size used by the current step                  */
+  double dtmin;   /* min over cells/dims of delta/(|u|+c) for the next step */
+  double cfl;     /* > 0: dt = min(cfl*dtmin, t_end - t); else dt fixed  */
+  double t_end;   /* > 0: clamp the last step to end at t_end            */
+  int64_t step;   /* completed steps                                     */
+} SwcClock;
+
+/* Library and error reporting. */
+int swc_abi_version(void);
+int swc_last_error(char* buf, size_t len);
+/* Number of this library's kernel launches issued by the calling thread. */
+int64_t swc_launch_count(void);
+
+/* Halo fill of `nfields` fields, dims in order x, y, z, for a single
+ * replica (boundary.py:34-86, 464-539; boundary.update_boundary :606-629).
+ * Fields with via_primitive are filled after rho (index rho_index) is
+ * complete. Replaces swirl_lm halo_exchange.inplace_halo_exchange as called
+ * from boundary.py:77-86. */
+int swc_halo_fill(const SwcGrid* grid, int32_t dtype, int32_t nfields,
+                  void* const* fields, const SwcFieldBC* bcs,
+                  int32_t rho_index, void* stream);
+
+/* One fused pass: RHS of the conserved state `uk` (halos already filled)
+ * followed by the stage combination selected by `mode`. `u0` may be NULL
+ * for SWC_OUT_RHS / SWC_OUT_EULER; `uout` may alias `u0` (pointwise) but
+ * never `uk`. `dt` is a device double; `dtmin_out`, when not NULL, is a
+ * device double min-reduced (atomically) with the CFL limit of `uout`.
+ * Interior cells of `uout` are written; its halos are left untouched.
+ * Replaces the rhs of get_rhs_fn (compressible_navier_stokes.py:68-268)
+ * and one stage of rk3.integrate / rk2.integrate (rk3.py:87-120,
+ * rk2.py:69-86). */
+int swc_rk_stage(const SwcGrid* grid, const SwcScheme* scheme,
+                 const void* const* uk, const void* const* u0,
+                 void* const* uout, int32_t mode, double c0, double c1,
+                 const double* dt, double* dtmin_out, void* stream);
+
+/* dtmin_out <- min(dtmin_out, min over interior cells and dims of
+ * delta_d / (|u_d| + c)), c = sqrt(gamma p / rho) (CFL rule of the
+ * reference's prototype, demo/swirl_c_prototype.ipynb `solve`). */
+int swc_cfl_reduce(const SwcGrid* grid, const SwcScheme* scheme,
+                   const void* const* u, double* dtmin_out, void* stream);
+
+/* Start of a step: clock->dt = cfl>0 ? min(cfl*dtmin, t_end-t) : dt;
+ * resets clock->dtmin to +inf for the coming reduction. */
+int swc_clock_begin_step(SwcClock* clock_dev, void* stream);
+/* End of a step: t += dt, step += 1. */
+int swc_clock_end_step(SwcClock* clock_dev, void* stream);
+
+/* Component kernels behind the reference's unit-level API. */
+
+/* Face reconstruction of one 3-D field along `dim` (0=x,1=y,2=z):
+ * neg/pos at face i-1/2 (swirl_lm interpolation.weno(v, dim, k) and
+ * flux_limiter(v, dim, MUSCL) as called at
+ * compressible_navier_stokes.py:581-589). */
+int swc_reconstruct(const SwcGrid* grid, int32_t dtype, int32_t interp,
+                    int32_t limiter, int32_t dim, const void* v, void* neg,
+                    void* pos, void* stream);
+
+/* Pointwise intercell convective flux for `n` face points from reconstructed
+ * primitive states. prim_neg/prim_pos hold 7 + nscalars arrays each:
+ * rho, u, v, w, e, p, h, scalars. p_dyn_neg/pos may be NULL (helper p_dyn,
+ * hllc.py:105-120). `pe` (n entries, may be NULL) is the potential energy
+ * at the face index. flux holds 5 + nscalars outputs.
+ * Replaces hll_convective_flux (hll.py:36-175) and hllc_convective_flux
+ * (hllc.py:33-257) with the physical flux of
+ * compressible_navier_stokes.py:338-427. */
+int swc_riemann_flux(int64_t n, int32_t dtype, int32_t riemann, int32_t dim,
+                     int32_t nscalars, const void* const* prim_neg,
+                     const void* const* prim_pos, const void* p_dyn_neg,
+                     const void* p_dyn_pos, const void* pe,
+                     void* const* flux, void* stream);
+
+/* Wave-speed estimates for `n` face points: s_l, s_r (hll.py:178-283) and,
+ * when s_m is not NULL, the HLLC contact speed (hllc.py:260-347). */
+int swc_wave_speeds(int64_t n, int32_t dtype, int32_t dim,
+                    const void* const* prim_neg, const void* const* prim_pos,
+                    const void* pe, void* s_l, void* s_m, void* s_r,
+                    void* stream);
+
+/* Stencils on a full 3-D array along `dim`: op 0 forward_1, 1 backward_1,
+ * 2 central_2 (gradient.py:21-94), 3 linear_interpolation
+ * (interpolation.py:21-53). Points whose stencil leaves the array get 0. */
+int swc_stencil(const SwcGrid* grid, int32_t dtype, int32_t op, int32_t dim,
+                double h, const void* f, void* out, void* stream);
+
+/* Stage algebra for a user-supplied rhs function, elementwise over `n`
+ * entries with the modes of swc_rk_stage (rk3.py:69-83, rk2.py:67-86):
+ * EULER: out = uk + l*dt; CONVEX: out = u0*c0 + (uk + l*dt)*c1;
+ * AVERAGE: out = c0*(u0 + (uk + dt*l)). `dt` is a device double. */
+int swc_rk_combine(int64_t n, int32_t dtype, int32_t mode, double c0,
+                   double c1, const double* dt, const void* u0,
+                   const void* uk, const void* l, void* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SWIRLC_B200_H_ */

@@ -1,0 +1,730 @@
+// C-ABI entry points of libswirlc_b200 (declared in include/swirlc_b200.h)
+// and the small kernels behind them: halo fill, CFL reduction, device clock,
+// and the unit-level kernels (reconstruction, pointwise Riemann flux, wave
+// speeds, stencils, stage algebra).
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+
+#include "swc_launch.h"
+#include "swirlc_b200.h"
+
+namespace swc {
+
+static thread_local std::string g_last_error;
+static thread_local int64_t g_launches = 0;
+
+void note_launch(int n) { g_launches += n; }
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+static int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return fail(SWC_ERR_LAUNCH, "%s: %s", what, cudaGetErrorString(e));
+  return SWC_OK;
+}
+
+static int check_grid(const SwcGrid* g) {
+  if (!g) return fail(SWC_ERR_ARG, "grid is NULL");
+  if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || g->halo < 0)
+    return fail(SWC_ERR_ARG, "bad grid sizes nx=%d ny=%d nz=%d halo=%d", g->nx,
+                g->ny, g->nz, g->halo);
+  const int64_t nya = g->ny + 2 * g->halo, nxa = g->nx + 2 * g->halo;
+  if (g->sx < nya || g->sz < g->sx * nxa)
+    return fail(SWC_ERR_ARG, "bad strides sx=%lld sz=%lld", (long long)g->sx,
+                (long long)g->sz);
+  return SWC_OK;
+}
+
+static bool dtype_ok(int d) { return d == SWC_F32 || d == SWC_F64; }
+
+// ---------------------------------------------------------------------------
+// Halo fill (boundary.py:34-86, 464-539).
+// ---------------------------------------------------------------------------
+struct HaloField {
+  void* f;
+  int via_prim;
+  SwcBC bc[2];
+};
+struct HaloArgs {
+  int dim;  // 0 x, 1 y, 2 z
+  int nf;
+  HaloField fld[SWC_MAX_FIELDS];
+  const void* rho;
+  int nx, ny, nz, h;
+  long long sx, sz;
+};
+
+template <typename T>
+__global__ void halo_kernel(const HaloArgs a) {
+  // Axis sizes with halos, storage order (z, x, y).
+  const int ext[3] = {a.nx + 2 * a.h, a.ny + 2 * a.h, a.nz + 2 * a.h};
+  const long long stride[3] = {a.sx, 1, a.sz};
+  const int d = a.dim;
+  // Plane axes (A, B) in storage order of the two other axes.
+  int ax_a, ax_b;
+  if (d == 0) { ax_a = 2; ax_b = 1; }
+  else if (d == 1) { ax_a = 2; ax_b = 0; }
+  else { ax_a = 0; ax_b = 1; }
+  const int na = ext[ax_a], nb = ext[ax_b];
+  const long long plane = (long long)na * nb;
+  const long long total = plane * 2 * a.nf;
+  const int n = ext[d] - 2 * a.h;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+       t < total; t += (long long)gridDim.x * blockDim.x) {
+    const long long pb = t % plane;
+    const int side = (int)((t / plane) % 2);
+    const int fi = (int)(t / (plane * 2));
+    const int ia = (int)(pb / nb), ib = (int)(pb % nb);
+    const long long base = ia * stride[ax_a] + ib * stride[ax_b];
+    const long long sd = stride[d];
+    T* f = static_cast<T*>(a.fld[fi].f);
+    const T* rho = static_cast<const T*>(a.rho);
+    const bool prim = a.fld[fi].via_prim != 0;
+    const SwcBC bc = a.fld[fi].bc[side];
+    auto pv = [&](long long o) -> T {  // value the BC acts on
+      if (!prim) return f[o];
+      T r = rho[o];
+      return r == T(0) ? T(0) : f[o] / r;
+    };
+    auto put = [&](long long o, T val) { f[o] = prim ? rho[o] * val : val; };
+    if (bc.kind == SWC_BC_PERIODIC) {
+      for (int l = 0; l < a.h; ++l) {
+        if (side == 0) put(base + l * sd, pv(base + (long long)(l + n) * sd));
+        else put(base + (long long)(n + a.h + l) * sd, pv(base + (long long)(a.h + l) * sd));
+      }
+    } else if (bc.kind == SWC_BC_DIRICHLET) {
+      const T* pl = static_cast<const T*>(bc.planes);
+      for (int l = 0; l < a.h; ++l) {
+        T val = bc.per_layer ? pl[l * plane + pb] : T(bc.value);
+        long long o = side == 0 ? base + l * sd : base + (long long)(n + a.h + l) * sd;
+        put(o, val);
+      }
+    } else if (bc.kind == SWC_BC_NEUMANN) {
+      const T inc = T(bc.value);
+      if (side == 0) {
+        T v = pv(base + (long long)a.h * sd);
+        for (int l = 0; l < a.h; ++l) {
+          v = v - inc;
+          put(base + (long long)(a.h - 1 - l) * sd, v);
+        }
+      } else {
+        T v = pv(base + (long long)(n + a.h - 1) * sd);
+        for (int l = 0; l < a.h; ++l) {
+          v = v + inc;
+          put(base + (long long)(n + a.h + l) * sd, v);
+        }
+      }
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// CFL reduction, device clock.
+// ---------------------------------------------------------------------------
+struct CflArgs {
+  const void* u[5];
+  const void* pe[3];
+  int has_pe;
+  int nx, ny, nz, h;
+  long long sx, sz;
+  double dx, dy, dz;
+  double* out;
+};
+
+template <typename T>
+__global__ void cfl_kernel(const CflArgs a) {
+  const long long n = (long long)a.nx * a.ny * a.nz;
+  double m = 1e300;
+  const T* u0 = static_cast<const T*>(a.u[0]);
+  const T* u1 = static_cast<const T*>(a.u[1]);
+  const T* u2 = static_cast<const T*>(a.u[2]);
+  const T* u3 = static_cast<const T*>(a.u[3]);
+  const T* u4 = static_cast<const T*>(a.u[4]);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(t % a.ny);
+    const int x = (int)((t / a.ny) % a.nx);
+    const int z = (int)(t / ((long long)a.ny * a.nx));
+    const int xa = x + a.h, ya = y + a.h, za = z + a.h;
+    const long long o = za * a.sz + xa * a.sx + ya;
+    T pe = T(0);
+    if (a.has_pe) {
+      const T* px = static_cast<const T*>(a.pe[0]);
+      const T* py = static_cast<const T*>(a.pe[1]);
+      const T* pz = static_cast<const T*>(a.pe[2]);
+      pe = (-(px ? px[xa] : T(0)) - (py ? py[ya] : T(0))) - (pz ? pz[za] : T(0));
+    }
+    T uu, vv, ww, e, p, hh;
+    T r = u0[o];
+    cons_to_prim(r, u1[o], u2[o], u3[o], u4[o], pe, uu, vv, ww, e, p, hh);
+    T c = sqrt_(K<T>::gamma() * p / r);
+    T l = min_(min_(T(a.dx) / (abs_(uu) + c), T(a.dy) / (abs_(vv) + c)),
+               T(a.dz) / (abs_(ww) + c));
+    m = fmin(m, double(l));
+  }
+  __shared__ double red[32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+    m = fmin(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = (threadIdx.x < blockDim.x / 32) ? red[threadIdx.x] : 1e300;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      m = fmin(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if (threadIdx.x == 0 && m < 1e300) atomic_min_pos(a.out, m);
+  }
+}
+
+__global__ void clock_begin_kernel(SwcClock* c) {
+  if (c->cfl > 0.0) {
+    double dt = c->cfl * c->dtmin;
+    if (c->t_end > 0.0) dt = fmin(dt, c->t_end - c->t);
+    c->dt = dt;
+  }
+  c->dtmin = 1e300;
+}
+
+__global__ void clock_end_kernel(SwcClock* c) {
+  c->t += c->dt;
+  c->step += 1;
+}
+
+// ---------------------------------------------------------------------------
+// Unit-level kernels.
+// ---------------------------------------------------------------------------
+struct Geo3 {
+  int nxa, nya, nza;  // extents with halos
+  long long sx, sz;
+};
+
+__device__ __forceinline__ void unflat(const Geo3& g, long long t, int& x,
+                                       int& y, int& z) {
+  y = (int)(t % g.nya);
+  x = (int)((t / g.nya) % g.nxa);
+  z = (int)(t / ((long long)g.nya * g.nxa));
+}
+
+template <typename T, int S>
+__global__ void recon_kernel(Geo3 g, int dim, int limiter, const T* v, T* neg,
+                             T* pos) {
+  constexpr int LO = Stencil<S>::LO, RI = Stencil<S>::RI;
+  const long long n = (long long)g.nxa * g.nya * g.nza;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int x, y, z;
+    unflat(g, t, x, y, z);
+    const int idx = dim == 0 ? x : (dim == 1 ? y : z);
+    const int ext = dim == 0 ? g.nxa : (dim == 1 ? g.nya : g.nza);
+    const long long st = dim == 0 ? g.sx : (dim == 1 ? 1 : g.sz);
+    const long long o = z * g.sz + x * g.sx + y;
+    if (idx - LO < 0 || idx + RI - 1 >= ext) {
+      neg[o] = T(0);
+      pos[o] = T(0);
+      continue;
+    }
+    T s[LO + RI];
+#pragma unroll
+    for (int k = 0; k < LO + RI; ++k) s[k] = v[o + (k - LO) * st];
+    T a, b;
+    reconstruct<S>(s, limiter, a, b);
+    neg[o] = a;
+    pos[o] = b;
+  }
+}
+
+struct PointArgs {
+  long long n;
+  const void* ql[7];
+  const void* qr[7];
+  const void* pdl;
+  const void* pdr;
+  const void* pe;
+  void* out[5];
+  void* sl;
+  void* sm;
+  void* sr;
+};
+
+template <typename T, int D>
+__device__ __forceinline__ void load_prim(const void* const* q, long long i,
+                                          Prim<T>& p) {
+  p.r = static_cast<const T*>(q[0])[i];
+  p.u[0] = static_cast<const T*>(q[1])[i];
+  p.u[1] = static_cast<const T*>(q[2])[i];
+  p.u[2] = static_cast<const T*>(q[3])[i];
+  p.e = static_cast<const T*>(q[4])[i];
+  p.p = static_cast<const T*>(q[5])[i];
+  p.h = static_cast<const T*>(q[6])[i];
+}
+
+template <typename T, int RM, int D>
+__global__ void riemann_kernel(const PointArgs a) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.n;
+       i += (long long)gridDim.x * blockDim.x) {
+    Prim<T> l, r;
+    load_prim<T, D>(a.ql, i, l);
+    load_prim<T, D>(a.qr, i, r);
+    T pdl = a.pdl ? static_cast<const T*>(a.pdl)[i] : l.p;
+    T pdr = a.pdr ? static_cast<const T*>(a.pdr)[i] : r.p;
+    T pe = a.pe ? static_cast<const T*>(a.pe)[i] : T(0);
+    T f[5];
+    if constexpr (RM == 0) hll_flux<T, D>(l, r, pdl, pdr, pe, f);
+    else hllc_flux<T, D>(l, r, pdl, pdr, pe, f);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) static_cast<T*>(a.out[k])[i] = f[k];
+  }
+}
+
+template <typename T, int D>
+__global__ void speeds_kernel(const PointArgs a) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.n;
+       i += (long long)gridDim.x * blockDim.x) {
+    Prim<T> l, r;
+    load_prim<T, D>(a.ql, i, l);
+    load_prim<T, D>(a.qr, i, r);
+    T pe = a.pe ? static_cast<const T*>(a.pe)[i] : T(0);
+    T s_l, s_r;
+    hll_speeds<T, D>(l, r, pe, s_l, s_r);
+    static_cast<T*>(a.sl)[i] = s_l;
+    static_cast<T*>(a.sr)[i] = s_r;
+    if (a.sm) static_cast<T*>(a.sm)[i] = hllc_contact<T, D>(l, r, s_l, s_r);
+  }
+}
+
+template <typename T>
+__global__ void stencil_kernel(Geo3 g, int op, int dim, double hd, const T* f,
+                               T* out) {
+  const long long n = (long long)g.nxa * g.nya * g.nza;
+  const T h = T(hd);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int x, y, z;
+    unflat(g, t, x, y, z);
+    const int idx = dim == 0 ? x : (dim == 1 ? y : z);
+    const int ext = dim == 0 ? g.nxa : (dim == 1 ? g.nya : g.nza);
+    const long long st = dim == 0 ? g.sx : (dim == 1 ? 1 : g.sz);
+    const long long o = z * g.sz + x * g.sx + y;
+    const bool has_m = idx - 1 >= 0, has_p = idx + 1 < ext;
+    T r = T(0);
+    if (op == 0) { if (has_p) r = (f[o + st] - f[o]) / h; }
+    else if (op == 1) { if (has_m) r = (f[o] - f[o - st]) / h; }
+    else if (op == 2) { if (has_m && has_p) r = (f[o + st] - f[o - st]) / (T(2) * h); }
+    else { if (has_m) r = T(0.5) * (f[o - st] + f[o]); }
+    out[o] = r;
+  }
+}
+
+template <typename T>
+__global__ void combine_kernel(long long n, int mode, double c0d, double c1d,
+                               const double* dtp, const T* u0, const T* uk,
+                               const T* l, T* out) {
+  const T dt = T(*dtp), c0 = T(c0d), c1 = T(c1d);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    T r;
+    if (mode == SWC_OUT_EULER) r = uk[i] + l[i] * dt;
+    else if (mode == SWC_OUT_CONVEX) r = u0[i] * c0 + (uk[i] + l[i] * dt) * c1;
+    else r = c0 * (u0[i] + (uk[i] + dt * l[i]));
+    out[i] = r;
+  }
+}
+
+static unsigned blocks_for(long long n, int threads = 256) {
+  long long b = (n + threads - 1) / threads;
+  return (unsigned)std::max<long long>(1, std::min<long long>(b, 148 * 32));
+}
+
+}  // namespace swc
+
+using namespace swc;
+
+extern "C" {
+
+int swc_abi_version(void) { return SWC_ABI_VERSION; }
+
+int swc_last_error(char* buf, size_t len) {
+  if (!buf || len == 0) return (int)g_last_error.size();
+  size_t n = std::min(len - 1, g_last_error.size());
+  memcpy(buf, g_last_error.data(), n);
+  buf[n] = 0;
+  return (int)n;
+}
+
+int64_t swc_launch_count(void) { return g_launches; }
+
+int swc_halo_fill(const SwcGrid* grid, int32_t dtype, int32_t nfields,
+                  void* const* fields, const SwcFieldBC* bcs,
+                  int32_t rho_index, void* stream) {
+  int st = check_grid(grid);
+  if (st) return st;
+  if (!dtype_ok(dtype)) return fail(SWC_ERR_ARG, "bad dtype %d", dtype);
+  if (nfields <= 0 || nfields > SWC_MAX_FIELDS || !fields || !bcs)
+    return fail(SWC_ERR_ARG, "bad field list (n=%d)", nfields);
+  bool any_prim = false;
+  for (int i = 0; i < nfields; ++i) {
+    if (!fields[i]) return fail(SWC_ERR_ARG, "field %d is NULL", i);
+    if (bcs[i].via_primitive) any_prim = true;
+    for (int d = 0; d < 3; ++d)
+      for (int s = 0; s < 2; ++s) {
+        const SwcBC& b = bcs[i].side[d][s];
+        if (b.kind != SWC_BC_PERIODIC && b.kind != SWC_BC_DIRICHLET &&
+            b.kind != SWC_BC_NEUMANN && b.kind != SWC_BC_NONE)
+          return fail(SWC_ERR_UNSUPPORTED, "Unsupported BC type %d.", b.kind);
+        if (b.kind == SWC_BC_DIRICHLET && b.per_layer && !b.planes)
+          return fail(SWC_ERR_ARG, "per-layer Dirichlet without planes");
+      }
+  }
+  if (any_prim && (rho_index < 0 || rho_index >= nfields))
+    return fail(SWC_ERR_ARG, "primitive BC needs rho (index %d)", rho_index);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int h = grid->halo;
+  if (h == 0) return SWC_OK;
+  // Phase 0: fields with direct BCs; phase 1: fields with primitive BCs,
+  // after rho is complete in all three dims.
+  for (int phase = 0; phase < (any_prim ? 2 : 1); ++phase) {
+    for (int d = 0; d < 3; ++d) {
+      HaloArgs a;
+      memset(&a, 0, sizeof(a));
+      a.dim = d;
+      a.nx = grid->nx; a.ny = grid->ny; a.nz = grid->nz; a.h = h;
+      a.sx = grid->sx; a.sz = grid->sz;
+      a.rho = any_prim ? fields[rho_index] : nullptr;
+      for (int i = 0; i < nfields; ++i) {
+        if ((bcs[i].via_primitive != 0) != (phase == 1)) continue;
+        const SwcBC& lo = bcs[i].side[d][0];
+        const SwcBC& hi = bcs[i].side[d][1];
+        if (lo.kind == SWC_BC_NONE && hi.kind == SWC_BC_NONE) continue;
+        HaloField& hf = a.fld[a.nf++];
+        hf.f = fields[i];
+        hf.via_prim = bcs[i].via_primitive;
+        // A periodic side makes the whole dim periodic (boundary.py:65-68).
+        if (lo.kind == SWC_BC_PERIODIC || hi.kind == SWC_BC_PERIODIC) {
+          hf.bc[0] = lo; hf.bc[1] = hi;
+          hf.bc[0].kind = hf.bc[1].kind = SWC_BC_PERIODIC;
+        } else {
+          hf.bc[0] = lo; hf.bc[1] = hi;
+        }
+      }
+      if (a.nf == 0) continue;
+      const int ext[3] = {grid->nx + 2 * h, grid->ny + 2 * h, grid->nz + 2 * h};
+      long long plane = (long long)ext[(d + 1) % 3] * ext[(d + 2) % 3];
+      long long total = plane * 2 * a.nf;
+      int threads = 256;
+      long long blocks = std::min<long long>((total + threads - 1) / threads, 148 * 16);
+      if (dtype == SWC_F32)
+        halo_kernel<float><<<(unsigned)blocks, threads, 0, s>>>(a);
+      else
+        halo_kernel<double><<<(unsigned)blocks, threads, 0, s>>>(a);
+      note_launch();
+      if ((st = check_launch("halo_fill"))) return st;
+    }
+  }
+  return SWC_OK;
+}
+
+int swc_rk_stage(const SwcGrid* grid, const SwcScheme* sc,
+                 const void* const* uk, const void* const* u0,
+                 void* const* uout, int32_t mode, double c0, double c1,
+                 const double* dt, double* dtmin_out, void* stream) {
+  int st = check_grid(grid);
+  if (st) return st;
+  if (!sc) return fail(SWC_ERR_ARG, "scheme is NULL");
+  if (!dtype_ok(sc->dtype)) return fail(SWC_ERR_ARG, "bad dtype %d", sc->dtype);
+  if (sc->interp < 0 || sc->interp > 3)
+    return fail(SWC_ERR_UNSUPPORTED, "interpolation scheme %d is not implemented", sc->interp);
+  if (sc->riemann != SWC_HLL && sc->riemann != SWC_HLLC)
+    return fail(SWC_ERR_ARG, "numeric flux scheme %d is not implemented", sc->riemann);
+  if (sc->nscalars != 0)
+    return fail(SWC_ERR_UNSUPPORTED, "transported scalars are not supported by the fused stage");
+  if (mode < SWC_OUT_RHS || mode > SWC_OUT_AVERAGE)
+    return fail(SWC_ERR_ARG, "bad stage mode %d", mode);
+  if (!uk || !uout) return fail(SWC_ERR_ARG, "NULL field list");
+  for (int v = 0; v < 5; ++v) {
+    if (!uk[v] || !uout[v]) return fail(SWC_ERR_ARG, "NULL field %d", v);
+    if (uout[v] == uk[v]) return fail(SWC_ERR_ARG, "uout must not alias uk");
+    if ((mode == SWC_OUT_CONVEX || mode == SWC_OUT_AVERAGE) && (!u0 || !u0[v]))
+      return fail(SWC_ERR_ARG, "stage mode %d needs u0", mode);
+  }
+  if (mode != SWC_OUT_RHS && !dt) return fail(SWC_ERR_ARG, "dt is NULL");
+  const int visc = sc->diffusion ? 1 : 0;
+  const int need = stage_halo_needed(sc->interp, visc);
+  if (grid->halo < need)
+    return fail(SWC_ERR_ARG, "halo_width %d is too small for this scheme (needs %d)",
+                grid->halo, need);
+  StageArgs a;
+  memset(&a, 0, sizeof(a));
+  a.nx = grid->nx; a.ny = grid->ny; a.nz = grid->nz; a.halo = grid->halo;
+  a.sx = grid->sx; a.sz = grid->sz;
+  a.dx = grid->dx; a.dy = grid->dy; a.dz = grid->dz;
+  for (int v = 0; v < 5; ++v) {
+    a.uk[v] = uk[v];
+    a.u0[v] = u0 ? u0[v] : nullptr;
+    a.uout[v] = uout[v];
+  }
+  a.mode = mode; a.c0 = c0; a.c1 = c1; a.dt = dt; a.dtmin_out = dtmin_out;
+  for (int d = 0; d < 3; ++d) {
+    a.pe[d] = sc->pe_axis[d];
+    if (sc->pe_axis[d]) a.has_pe = 1;
+    a.g[d] = sc->g[d];
+  }
+  a.limiter = sc->limiter;
+  a.nu = sc->nu; a.pr = sc->pr > 0 ? sc->pr : 1.0;
+  a.gravity_mask = sc->gravity_mask;
+  // z segment per CTA: enough CTAs for ~4 waves of 2 CTAs/SM, >= 8 planes.
+  int zseg = sc->zseg;
+  if (zseg <= 0) {
+    long long tiles2d = (long long)((grid->ny + 31) / 32) * ((grid->nx + 7) / 8);
+    long long nseg = std::max<long long>(1, (148 * 2 * 4 + tiles2d - 1) / tiles2d);
+    zseg = (int)std::max<long long>(8, (grid->nz + nseg - 1) / nseg);
+  }
+  a.zseg = std::min(zseg, grid->nz);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int tile = sc->tile;
+  int rc;
+  if (sc->dtype == SWC_F32) {
+    switch (sc->interp) {
+      case 0: rc = launch_stage_f32_s0(a, sc->riemann, visc, tile, s); break;
+      case 1: rc = launch_stage_f32_s1(a, sc->riemann, visc, tile, s); break;
+      case 2: rc = launch_stage_f32_s2(a, sc->riemann, visc, tile, s); break;
+      default: rc = launch_stage_f32_s3(a, sc->riemann, visc, tile, s); break;
+    }
+  } else {
+    switch (sc->interp) {
+      case 0: rc = launch_stage_f64_s0(a, sc->riemann, visc, tile, s); break;
+      case 1: rc = launch_stage_f64_s1(a, sc->riemann, visc, tile, s); break;
+      case 2: rc = launch_stage_f64_s2(a, sc->riemann, visc, tile, s); break;
+      default: rc = launch_stage_f64_s3(a, sc->riemann, visc, tile, s); break;
+    }
+  }
+  if (rc) return fail(rc, "stage launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  return SWC_OK;
+}
+
+int swc_cfl_reduce(const SwcGrid* grid, const SwcScheme* sc,
+                   const void* const* u, double* dtmin_out, void* stream) {
+  int st = check_grid(grid);
+  if (st) return st;
+  if (!sc || !dtype_ok(sc->dtype)) return fail(SWC_ERR_ARG, "bad scheme/dtype");
+  if (!u || !dtmin_out) return fail(SWC_ERR_ARG, "NULL argument");
+  CflArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int v = 0; v < 5; ++v) {
+    if (!u[v]) return fail(SWC_ERR_ARG, "NULL field %d", v);
+    a.u[v] = u[v];
+  }
+  for (int d = 0; d < 3; ++d) {
+    a.pe[d] = sc->pe_axis[d];
+    if (sc->pe_axis[d]) a.has_pe = 1;
+  }
+  a.nx = grid->nx; a.ny = grid->ny; a.nz = grid->nz; a.h = grid->halo;
+  a.sx = grid->sx; a.sz = grid->sz;
+  a.dx = grid->dx; a.dy = grid->dy; a.dz = grid->dz;
+  a.out = dtmin_out;
+  long long n = (long long)grid->nx * grid->ny * grid->nz;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (sc->dtype == SWC_F32) cfl_kernel<float><<<blocks_for(n), 256, 0, s>>>(a);
+  else cfl_kernel<double><<<blocks_for(n), 256, 0, s>>>(a);
+  note_launch();
+  return check_launch("cfl_reduce");
+}
+
+int swc_clock_begin_step(SwcClock* clock_dev, void* stream) {
+  if (!clock_dev) return fail(SWC_ERR_ARG, "clock is NULL");
+  clock_begin_kernel<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(clock_dev);
+  note_launch();
+  return check_launch("clock_begin_step");
+}
+
+int swc_clock_end_step(SwcClock* clock_dev, void* stream) {
+  if (!clock_dev) return fail(SWC_ERR_ARG, "clock is NULL");
+  clock_end_kernel<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(clock_dev);
+  note_launch();
+  return check_launch("clock_end_step");
+}
+
+int swc_reconstruct(const SwcGrid* grid, int32_t dtype, int32_t interp,
+                    int32_t limiter, int32_t dim, const void* v, void* neg,
+                    void* pos, void* stream) {
+  int st = check_grid(grid);
+  if (st) return st;
+  if (!dtype_ok(dtype)) return fail(SWC_ERR_ARG, "bad dtype %d", dtype);
+  if (interp < 0 || interp > 3)
+    return fail(SWC_ERR_UNSUPPORTED, "interpolation scheme %d is not implemented", interp);
+  if (dim < 0 || dim > 2) return fail(SWC_ERR_ARG, "bad dim %d", dim);
+  if (!v || !neg || !pos) return fail(SWC_ERR_ARG, "NULL array");
+  Geo3 g{grid->nx + 2 * grid->halo, grid->ny + 2 * grid->halo,
+         grid->nz + 2 * grid->halo, grid->sx, grid->sz};
+  long long n = (long long)g.nxa * g.nya * g.nza;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+#define SWC_RECON(T, S)                                                     \
+  recon_kernel<T, S><<<blocks_for(n), 256, 0, s>>>(                         \
+      g, dim, limiter, static_cast<const T*>(v), static_cast<T*>(neg),      \
+      static_cast<T*>(pos))
+  if (dtype == SWC_F32) {
+    switch (interp) {
+      case 0: SWC_RECON(float, 0); break;
+      case 1: SWC_RECON(float, 1); break;
+      case 2: SWC_RECON(float, 2); break;
+      default: SWC_RECON(float, 3); break;
+    }
+  } else {
+    switch (interp) {
+      case 0: SWC_RECON(double, 0); break;
+      case 1: SWC_RECON(double, 1); break;
+      case 2: SWC_RECON(double, 2); break;
+      default: SWC_RECON(double, 3); break;
+    }
+  }
+#undef SWC_RECON
+  note_launch();
+  return check_launch("reconstruct");
+}
+
+static int point_args(int64_t n, const void* const* ql, const void* const* qr,
+                      const void* pe, PointArgs& a) {
+  memset(&a, 0, sizeof(a));
+  if (n < 0) return fail(SWC_ERR_ARG, "negative size");
+  if (!ql || !qr) return fail(SWC_ERR_ARG, "NULL state list");
+  for (int k = 0; k < 7; ++k) {
+    if (!ql[k] || !qr[k]) return fail(SWC_ERR_ARG, "NULL primitive %d", k);
+    a.ql[k] = ql[k];
+    a.qr[k] = qr[k];
+  }
+  a.n = n;
+  a.pe = pe;
+  return SWC_OK;
+}
+
+int swc_riemann_flux(int64_t n, int32_t dtype, int32_t riemann, int32_t dim,
+                     int32_t nscalars, const void* const* prim_neg,
+                     const void* const* prim_pos, const void* p_dyn_neg,
+                     const void* p_dyn_pos, const void* pe,
+                     void* const* flux, void* stream) {
+  if (!dtype_ok(dtype)) return fail(SWC_ERR_ARG, "bad dtype %d", dtype);
+  if (riemann != SWC_HLL && riemann != SWC_HLLC)
+    return fail(SWC_ERR_ARG, "numeric flux scheme %d is not implemented", riemann);
+  if (dim < 0 || dim > 2) return fail(SWC_ERR_ARG, "bad dim %d", dim);
+  if (nscalars != 0) return fail(SWC_ERR_UNSUPPORTED, "scalars not supported here");
+  PointArgs a;
+  int st = point_args(n, prim_neg, prim_pos, pe, a);
+  if (st) return st;
+  if ((p_dyn_neg == nullptr) != (p_dyn_pos == nullptr))
+    return fail(SWC_ERR_ARG, "p_dyn needs both sides");
+  a.pdl = p_dyn_neg;
+  a.pdr = p_dyn_pos;
+  if (!flux) return fail(SWC_ERR_ARG, "NULL flux list");
+  for (int k = 0; k < 5; ++k) {
+    if (!flux[k]) return fail(SWC_ERR_ARG, "NULL flux %d", k);
+    a.out[k] = flux[k];
+  }
+  if (n == 0) return SWC_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  unsigned b = blocks_for(n);
+#define SWC_RM(T, RM)                                                        \
+  switch (dim) {                                                             \
+    case 0: riemann_kernel<T, RM, 0><<<b, 256, 0, s>>>(a); break;           \
+    case 1: riemann_kernel<T, RM, 1><<<b, 256, 0, s>>>(a); break;           \
+    default: riemann_kernel<T, RM, 2><<<b, 256, 0, s>>>(a); break;          \
+  }
+  if (dtype == SWC_F32) {
+    if (riemann == SWC_HLL) { SWC_RM(float, 0) } else { SWC_RM(float, 1) }
+  } else {
+    if (riemann == SWC_HLL) { SWC_RM(double, 0) } else { SWC_RM(double, 1) }
+  }
+#undef SWC_RM
+  note_launch();
+  return check_launch("riemann_flux");
+}
+
+int swc_wave_speeds(int64_t n, int32_t dtype, int32_t dim,
+                    const void* const* prim_neg, const void* const* prim_pos,
+                    const void* pe, void* s_l, void* s_m, void* s_r,
+                    void* stream) {
+  if (!dtype_ok(dtype)) return fail(SWC_ERR_ARG, "bad dtype %d", dtype);
+  if (dim < 0 || dim > 2) return fail(SWC_ERR_ARG, "bad dim %d", dim);
+  PointArgs a;
+  int st = point_args(n, prim_neg, prim_pos, pe, a);
+  if (st) return st;
+  if (!s_l || !s_r) return fail(SWC_ERR_ARG, "NULL output");
+  a.sl = s_l; a.sm = s_m; a.sr = s_r;
+  if (n == 0) return SWC_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  unsigned b = blocks_for(n);
+#define SWC_SP(T)                                                            \
+  switch (dim) {                                                             \
+    case 0: speeds_kernel<T, 0><<<b, 256, 0, s>>>(a); break;                \
+    case 1: speeds_kernel<T, 1><<<b, 256, 0, s>>>(a); break;                \
+    default: speeds_kernel<T, 2><<<b, 256, 0, s>>>(a); break;               \
+  }
+  if (dtype == SWC_F32) { SWC_SP(float) } else { SWC_SP(double) }
+#undef SWC_SP
+  note_launch();
+  return check_launch("wave_speeds");
+}
+
+int swc_stencil(const SwcGrid* grid, int32_t dtype, int32_t op, int32_t dim,
+                double h, const void* f, void* out, void* stream) {
+  int st = check_grid(grid);
+  if (st) return st;
+  if (!dtype_ok(dtype)) return fail(SWC_ERR_ARG, "bad dtype %d", dtype);
+  if (op < 0 || op > 3) return fail(SWC_ERR_ARG, "bad stencil op %d", op);
+  if (dim < 0 || dim > 2)
+    return fail(SWC_ERR_ARG, "\"%d\" is not a valid dimension.", dim);
+  if (!f || !out || f == out) return fail(SWC_ERR_ARG, "bad arrays");
+  Geo3 g{grid->nx + 2 * grid->halo, grid->ny + 2 * grid->halo,
+         grid->nz + 2 * grid->halo, grid->sx, grid->sz};
+  long long n = (long long)g.nxa * g.nya * g.nza;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (dtype == SWC_F32)
+    stencil_kernel<float><<<blocks_for(n), 256, 0, s>>>(
+        g, op, dim, h, static_cast<const float*>(f), static_cast<float*>(out));
+  else
+    stencil_kernel<double><<<blocks_for(n), 256, 0, s>>>(
+        g, op, dim, h, static_cast<const double*>(f), static_cast<double*>(out));
+  note_launch();
+  return check_launch("stencil");
+}
+
+int swc_rk_combine(int64_t n, int32_t dtype, int32_t mode, double c0,
+                   double c1, const double* dt, const void* u0,
+                   const void* uk, const void* l, void* out, void* stream) {
+  if (!dtype_ok(dtype)) return fail(SWC_ERR_ARG, "bad dtype %d", dtype);
+  if (mode != SWC_OUT_EULER && mode != SWC_OUT_CONVEX && mode != SWC_OUT_AVERAGE)
+    return fail(SWC_ERR_ARG, "bad combine mode %d", mode);
+  if (!dt || !uk || !l || !out || (mode != SWC_OUT_EULER && !u0))
+    return fail(SWC_ERR_ARG, "NULL argument");
+  if (n <= 0) return n == 0 ? SWC_OK : fail(SWC_ERR_ARG, "negative size");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (dtype == SWC_F32)
+    combine_kernel<float><<<blocks_for(n), 256, 0, s>>>(
+        n, mode, c0, c1, dt, static_cast<const float*>(u0),
+        static_cast<const float*>(uk), static_cast<const float*>(l),
+        static_cast<float*>(out));
+  else
+    combine_kernel<double><<<blocks_for(n), 256, 0, s>>>(
+        n, mode, c0, c1, dt, static_cast<const double*>(u0),
+        static_cast<const double*>(uk), static_cast<const double*>(l),
+        static_cast<double*>(out));
+  note_launch();
+  return check_launch("rk_combine");
+}
+
+}  // extern "C"

@@ -1,0 +1,40 @@
+// Host-side declarations shared by the C-ABI translation unit and the
+// per-(dtype, scheme) stage-kernel instantiation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "swc_stage.cuh"
+
+namespace swc {
+
+// Launches the fused stage kernel for one (dtype, scheme); returns 0 or a
+// negative SWC status. Defined in swc_stage_inst.cu, compiled once per pair.
+#define SWC_DECL_STAGE(SUFFIX)                                               \
+  int launch_stage_##SUFFIX(const StageArgs& a, int riemann, int visc,       \
+                            int tile, cudaStream_t st);                      \
+  size_t stage_smem_##SUFFIX(int visc, int tile);
+SWC_DECL_STAGE(f32_s0)
+SWC_DECL_STAGE(f32_s1)
+SWC_DECL_STAGE(f32_s2)
+SWC_DECL_STAGE(f32_s3)
+SWC_DECL_STAGE(f64_s0)
+SWC_DECL_STAGE(f64_s1)
+SWC_DECL_STAGE(f64_s2)
+SWC_DECL_STAGE(f64_s3)
+#undef SWC_DECL_STAGE
+
+// Halo layers the stage kernel needs for a scheme.
+inline int stage_halo_needed(int scheme, int visc) {
+  switch (scheme) {
+    case 0: return visc ? Geom<0, true>::NEED : Geom<0, false>::NEED;
+    case 1: return visc ? Geom<1, true>::NEED : Geom<1, false>::NEED;
+    case 2: return visc ? Geom<2, true>::NEED : Geom<2, false>::NEED;
+    default: return visc ? Geom<3, true>::NEED : Geom<3, false>::NEED;
+  }
+}
+
+// Counts kernel launches issued by this library (thread-local).
+void note_launch(int n = 1);
+
+}  // namespace swc

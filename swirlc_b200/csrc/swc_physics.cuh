@@ -1,0 +1,383 @@
+// Device-side physics of the Swirl-C compressible RHS, shared by the fused
+// stage kernel and the unit-level kernels.
+//
+// Each function states the reference lines it follows (paths relative to the
+// swirl_c project root). Arithmetic runs in T (float or double).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace swc {
+
+// physics/constant.py:17-41. Python doubles rounded once to T, as TF does
+// when it mixes a Python float with a float32 tensor.
+template <typename T>
+struct K {
+  static constexpr double kGamma = 1.4;
+  static constexpr double kR = 8.314 / 0.029;
+  static constexpr double kCv = kR / (kGamma - 1.0);
+  static constexpr double kCp = kCv + kR;
+  static constexpr double kG = 9.81;
+  __device__ static constexpr T gamma() { return T(kGamma); }
+  __device__ static constexpr T gm1() { return T(kGamma - 1.0); }
+  __device__ static constexpr T r_gas() { return T(kR); }
+  __device__ static constexpr T cp() { return T(kCp); }
+  __device__ static constexpr T grav() { return T(kG); }
+};
+
+template <typename T>
+__device__ __forceinline__ T dnn(T x, T y) {  // tf.math.divide_no_nan
+  return y == T(0) ? T(0) : x / y;
+}
+// Single precision is built with -use_fast_math: 1/x is the hardware
+// reciprocal approximation (<= 1 ulp) and x/y the 2-ulp division.
+__device__ __forceinline__ float rcp_(float x) { return 1.0f / x; }
+__device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
+__device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+__device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+__device__ __forceinline__ float min_(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double min_(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float max_(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double max_(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float abs_(float a) { return fabsf(a); }
+__device__ __forceinline__ double abs_(double a) { return fabs(a); }
+
+// Primitive state at a face or a cell: rho, (u, v, w), e, p, h.
+template <typename T>
+struct Prim {
+  T r;
+  T u[3];
+  T e, p, h;
+};
+
+// Cell primitives from conserved values (utils.py:145-183 multiplies by the
+// reciprocal of rho) and p, h (generic.py:27-87, 356-388).
+template <typename T>
+__device__ __forceinline__ void cons_to_prim(T rho, T ru, T rv, T rw, T re,
+                                             T pe, T& u, T& v, T& w, T& e,
+                                             T& p, T& h) {
+  T inv = T(1) / rho;
+  u = inv * ru;
+  v = inv * rv;
+  w = inv * rw;
+  e = inv * re;
+  T eint = e - T(0.5) * (u * u + v * v + w * w) - pe;
+  p = K<T>::gm1() * rho * eint;
+  h = e + p / rho;
+}
+
+// ---------------------------------------------------------------------------
+// Face reconstruction. A stencil s[0 .. LO+RI-1] holds the cell values
+// v[i-LO .. i+RI-1] around face i-1/2; neg comes from the left cell i-1,
+// pos from the right cell i (compressible_navier_stokes.py:597-615).
+// WENO-JS weights alpha_r = d_r / (eps + beta_r)^2 with eps = 1e-6 and the
+// candidate polynomials of the reference prototype
+// (demo/swirl_c_prototype.ipynb `weno5`, cell 4).
+// ---------------------------------------------------------------------------
+template <int SCHEME>
+struct Stencil;
+
+template <>
+struct Stencil<0> {  // WENO5
+  static constexpr int LO = 3, RI = 3;
+};
+template <>
+struct Stencil<1> {  // WENO3
+  static constexpr int LO = 2, RI = 2;
+};
+template <>
+struct Stencil<2> {  // MUSCL
+  static constexpr int LO = 2, RI = 2;
+};
+template <>
+struct Stencil<3> {  // NODE (identity)
+  static constexpr int LO = 0, RI = 1;
+};
+
+// WENO5 value on the right face (c+1/2) of cell c from v[c-2..c+2].
+template <typename T>
+__device__ __forceinline__ T weno5_right(T vm2, T vm1, T v0, T vp1, T vp2) {
+  const T c1312 = T(13.0 / 12.0), q = T(0.25), eps = T(1e-6);
+  T a = v0 - T(2) * vp1 + vp2, b = T(3) * v0 - T(4) * vp1 + vp2;
+  T b0 = c1312 * a * a + q * b * b;
+  a = vm1 - T(2) * v0 + vp1;
+  b = vm1 - vp1;
+  T b1 = c1312 * a * a + q * b * b;
+  a = vm2 - T(2) * vm1 + v0;
+  b = vm2 - T(4) * vm1 + T(3) * v0;
+  T b2 = c1312 * a * a + q * b * b;
+  b0 += eps;
+  b1 += eps;
+  b2 += eps;
+  T a0 = T(0.3) * rcp_(b0 * b0);
+  T a1 = T(0.6) * rcp_(b1 * b1);
+  T a2 = T(0.1) * rcp_(b2 * b2);
+  T q0 = T(1.0 / 3.0) * v0 + T(5.0 / 6.0) * vp1 - T(1.0 / 6.0) * vp2;
+  T q1 = T(-1.0 / 6.0) * vm1 + T(5.0 / 6.0) * v0 + T(1.0 / 3.0) * vp1;
+  T q2 = T(1.0 / 3.0) * vm2 - T(7.0 / 6.0) * vm1 + T(11.0 / 6.0) * v0;
+  return (a0 * q0 + a1 * q1 + a2 * q2) * rcp_(a0 + a1 + a2);
+}
+
+// WENO5 value on the left face (c-1/2) of cell c from v[c-2..c+2].
+template <typename T>
+__device__ __forceinline__ T weno5_left(T vm2, T vm1, T v0, T vp1, T vp2) {
+  const T c1312 = T(13.0 / 12.0), q = T(0.25), eps = T(1e-6);
+  T a = v0 - T(2) * vp1 + vp2, b = T(3) * v0 - T(4) * vp1 + vp2;
+  T b0 = c1312 * a * a + q * b * b;
+  a = vm1 - T(2) * v0 + vp1;
+  b = vm1 - vp1;
+  T b1 = c1312 * a * a + q * b * b;
+  a = vm2 - T(2) * vm1 + v0;
+  b = vm2 - T(4) * vm1 + T(3) * v0;
+  T b2 = c1312 * a * a + q * b * b;
+  b0 += eps;
+  b1 += eps;
+  b2 += eps;
+  T a0 = T(0.1) * rcp_(b0 * b0);
+  T a1 = T(0.6) * rcp_(b1 * b1);
+  T a2 = T(0.3) * rcp_(b2 * b2);
+  T q0 = T(11.0 / 6.0) * v0 - T(7.0 / 6.0) * vp1 + T(1.0 / 3.0) * vp2;
+  T q1 = T(1.0 / 3.0) * vm1 + T(5.0 / 6.0) * v0 - T(1.0 / 6.0) * vp1;
+  T q2 = T(-1.0 / 6.0) * vm2 + T(5.0 / 6.0) * vm1 + T(1.0 / 3.0) * v0;
+  return (a0 * q0 + a1 * q1 + a2 * q2) * rcp_(a0 + a1 + a2);
+}
+
+// WENO3 (k = 2) right / left face values of cell c from v[c-1..c+1], with
+// d = (2/3, 1/3) and candidates c[-1..1] = (3/2,-1/2), (1/2,1/2), (-1/2,3/2).
+template <typename T>
+__device__ __forceinline__ T weno3_right(T vm1, T v0, T vp1) {
+  const T eps = T(1e-6);
+  T b0 = (vp1 - v0) * (vp1 - v0) + eps;
+  T b1 = (v0 - vm1) * (v0 - vm1) + eps;
+  T a0 = T(2.0 / 3.0) * rcp_(b0 * b0);
+  T a1 = T(1.0 / 3.0) * rcp_(b1 * b1);
+  T q0 = T(0.5) * v0 + T(0.5) * vp1;
+  T q1 = T(-0.5) * vm1 + T(1.5) * v0;
+  return (a0 * q0 + a1 * q1) * rcp_(a0 + a1);
+}
+template <typename T>
+__device__ __forceinline__ T weno3_left(T vm1, T v0, T vp1) {
+  const T eps = T(1e-6);
+  T b0 = (vp1 - v0) * (vp1 - v0) + eps;
+  T b1 = (v0 - vm1) * (v0 - vm1) + eps;
+  T a0 = T(1.0 / 3.0) * rcp_(b0 * b0);
+  T a1 = T(2.0 / 3.0) * rcp_(b1 * b1);
+  T q0 = T(1.5) * v0 - T(0.5) * vp1;
+  T q1 = T(0.5) * vm1 + T(0.5) * v0;
+  return (a0 * q0 + a1 * q1) * rcp_(a0 + a1);
+}
+
+// MUSCL slope of cell c: phi(r) * dp with r = dnn(dm, dp).
+template <typename T>
+__device__ __forceinline__ T muscl_slope(T vm1, T v0, T vp1, int limiter) {
+  T dp = vp1 - v0, dm = v0 - vm1;
+  T r = dnn(dm, dp);
+  T phi;
+  if (limiter == 0) {  // van Leer
+    T a = abs_(r);
+    phi = (r + a) / (T(1) + a);
+  } else if (limiter == 1) {  // monotonized central
+    phi = max_(T(0), min_(min_(T(2) * r, T(0.5) * (T(1) + r)), T(2)));
+  } else {  // minmod
+    phi = max_(T(0), min_(r, T(1)));
+  }
+  return phi * dp;
+}
+
+template <int SCHEME, typename T>
+__device__ __forceinline__ void reconstruct(const T* s, int limiter, T& neg,
+                                            T& pos) {
+  if constexpr (SCHEME == 0) {
+    neg = weno5_right(s[0], s[1], s[2], s[3], s[4]);
+    pos = weno5_left(s[1], s[2], s[3], s[4], s[5]);
+  } else if constexpr (SCHEME == 1) {
+    neg = weno3_right(s[0], s[1], s[2]);
+    pos = weno3_left(s[1], s[2], s[3]);
+  } else if constexpr (SCHEME == 2) {
+    neg = s[1] + T(0.5) * muscl_slope(s[0], s[1], s[2], limiter);
+    pos = s[2] - T(0.5) * muscl_slope(s[1], s[2], s[3], limiter);
+  } else {
+    neg = s[0];
+    pos = s[0];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Riemann solvers.
+// ---------------------------------------------------------------------------
+// Physical flux along D of one face state (compressible_navier_stokes.py:
+// 338-427): mass m = rho*u_D; momentum m*u_i (+ p_upd when i == D); energy
+// m*(e + p/rho) with the full p.
+template <typename T, int D>
+__device__ __forceinline__ void physical_flux(const Prim<T>& q, T p_upd,
+                                              T* f) {
+  T m = q.r * q.u[D];
+  f[0] = m;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) f[1 + i] = m * q.u[i];
+  f[1 + D] = f[1 + D] + p_upd;
+  f[4] = m * (q.e + q.p / q.r);
+}
+
+// Roe-averaged wave-speed estimates (hll.py:178-283): c = sqrt(gamma p/rho)
+// per side, Roe averages with sqrt(rho) weights and reciprocal_no_nan,
+// c~ from the sensible enthalpy with the potential energy pe of the cell at
+// the face index (generic.py:144-148, 391-423).
+template <typename T, int D>
+__device__ __forceinline__ void hll_speeds(const Prim<T>& l, const Prim<T>& r,
+                                           T pe, T& s_l, T& s_r) {
+  T c_l = sqrt_(K<T>::gamma() * l.p / l.r);
+  T c_r = sqrt_(K<T>::gamma() * r.p / r.r);
+  T rl = sqrt_(l.r), rr = sqrt_(r.r);
+  T den = rl + rr;
+  T inv = den == T(0) ? T(0) : T(1) / den;
+  T ru[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) ru[i] = (rl * l.u[i] + rr * r.u[i]) * inv;
+  T rh = (rl * l.h + rr * r.h) * inv;
+  T hs = rh - T(0.5) * (ru[0] * ru[0] + ru[1] * ru[1] + ru[2] * ru[2]) - pe;
+  T rc = sqrt_(K<T>::gm1() * hs);
+  s_l = min_(l.u[D] - c_l, ru[D] - rc);
+  s_r = max_(r.u[D] + c_r, ru[D] + rc);
+}
+
+// HLL flux (hll.py:107-170): F = t1 F_R + t2 F_L - t3 (U_R - U_L). The wave
+// speeds use the full pressure; pdl / pdr replace p in the aligned momentum
+// flux when the helper variable p_dyn is present
+// (compressible_navier_stokes.py:378).
+template <typename T, int D>
+__device__ __forceinline__ void hll_flux(const Prim<T>& l, const Prim<T>& r,
+                                         T pdl, T pdr, T pe, T* f) {
+  T s_l, s_r;
+  hll_speeds<T, D>(l, r, pe, s_l, s_r);
+  T ds = s_r - s_l;
+  T t1 = dnn(min_(s_r, T(0)) - min_(s_l, T(0)), ds);
+  T t2 = T(1) - t1;
+  T t3 = dnn(s_r * abs_(s_l) - s_l * abs_(s_r), T(2) * ds);
+  T fl[5], fr[5];
+  physical_flux<T, D>(l, pdl, fl);
+  physical_flux<T, D>(r, pdr, fr);
+  T ul[5] = {l.r, l.r * l.u[0], l.r * l.u[1], l.r * l.u[2], l.r * l.e};
+  T ur[5] = {r.r, r.r * r.u[0], r.r * r.u[1], r.r * r.u[2], r.r * r.e};
+#pragma unroll
+  for (int k = 0; k < 5; ++k)
+    f[k] = t1 * fr[k] + t2 * fl[k] - t3 * (ur[k] - ul[k]);
+}
+
+// HLLC contact speed (hllc.py:328-341), zeroed when |s_m| < 1e-6.
+template <typename T, int D>
+__device__ __forceinline__ T hllc_contact(const Prim<T>& l, const Prim<T>& r,
+                                          T s_l, T s_r) {
+  T vl = l.u[D], vr = r.u[D];
+  T num = r.p - l.p + l.r * vl * (s_l - vl) - r.r * vr * (s_r - vr);
+  T den = l.r * (s_l - vl) - r.r * (s_r - vr);
+  T s_m = dnn(num, den);
+  return abs_(s_m) < T(1e-6) ? T(0) : s_m;
+}
+
+// HLLC flux (hllc.py:105-257). With p_dyn present, the wave speeds and the
+// star states use p = p_dyn (hllc.py:109-120) while the physical flux keeps
+// the full p in the energy flux. The four-way select of hllc.py:229-243
+// picks one side k and whether its star flux applies; only that side's flux
+// is evaluated (same value as evaluating all four and selecting).
+template <typename T, int D>
+__device__ __forceinline__ void hllc_flux(const Prim<T>& l, const Prim<T>& r,
+                                          T pdl, T pdr, T pe, T* f) {
+  Prim<T> lu = l, ru = r;
+  lu.p = pdl;
+  ru.p = pdr;
+  T s_l, s_r;
+  hll_speeds<T, D>(lu, ru, pe, s_l, s_r);
+  T s_m = hllc_contact<T, D>(lu, ru, s_l, s_r);
+  bool c1 = s_l >= T(0);
+  bool c2 = (s_l <= T(0)) && (s_m >= T(0));
+  bool c3 = (s_m <= T(0)) && (s_r >= T(0));
+  bool left = c1 || c2;
+  bool star = !c1 && (c2 || c3);
+  Prim<T> q;
+  q.r = left ? l.r : r.r;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) q.u[i] = left ? l.u[i] : r.u[i];
+  q.e = left ? l.e : r.e;
+  q.p = left ? l.p : r.p;
+  q.h = left ? l.h : r.h;
+  T pd = left ? pdl : pdr;
+  T s_k = left ? s_l : s_r;
+  physical_flux<T, D>(q, pd, f);
+  if (star) {
+    T v_k = q.u[D];
+    T rat = dnn(s_k, s_k - s_m);
+    T dv = s_m - v_k;
+    f[0] = f[0] + q.r * dv * rat;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (i == D) {
+        f[1 + i] = f[1 + i] + q.r * s_k * (dnn(s_k - v_k, s_k - s_m) * s_m - v_k);
+      } else {
+        f[1 + i] = f[1 + i] + q.r * dv * q.u[i] * rat;
+      }
+    }
+    f[4] = f[4] + q.r * rat * dv * (q.e + pd / q.r + (s_k - v_k) * s_m);
+  }
+}
+
+template <int RIEMANN, typename T, int D>
+__device__ __forceinline__ void riemann(const Prim<T>& l, const Prim<T>& r,
+                                        T pe, T* f) {
+  if constexpr (RIEMANN == 0) {
+    hll_flux<T, D>(l, r, l.p, r.p, pe, f);
+  } else {
+    hllc_flux<T, D>(l, r, l.p, r.p, pe, f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Viscous flux on the face between cells a (i-1) and b (i) along D
+// (compressible_navier_stokes.py:618-707; diffusion.py:33-109;
+// fluid.py:31-111). `ga[t][c]` / `gb[t][c]` are the central differences
+// (f[+1]-f[-1])/(2h_t) of velocity component c along tangential axis t at
+// cells a and b; only c == t and c == D are used.
+// ---------------------------------------------------------------------------
+template <typename T, int D>
+__device__ __forceinline__ void viscous_flux(
+    T ra, T rb, const T* ua, const T* ub, T pa, T pb, const T ga[3][3],
+    const T gb[3][3], T h_d, T nu, T inv_pr, T* f) {
+  // Backward differences along D of u, v, w and T = p/(rho R).
+  T bd[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) bd[c] = (ub[c] - ua[c]) / h_d;
+  // div on face D: bwd_D(u_D) + sum over t != D of lin(central_t(u_t)).
+  T g[3];  // g[c] = d u_c / d x_c on face D
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    g[c] = (c == D) ? bd[D] : T(0.5) * (ga[c][c] + gb[c][c]);
+  T div = g[0] + g[1] + g[2];
+  T rf = T(0.5) * (ra + rb);
+  T tau[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    T s;
+    if (c == D) {
+      s = bd[D] - T(1.0 / 3.0) * div;
+    } else {
+      // s_cD = 0.5 * (bwd_D(u_c) + lin_D(central_c(u_D)))
+      s = T(0.5) * (bd[c] + T(0.5) * (ga[c][D] + gb[c][D]));
+    }
+    tau[c] = T(2) * rf * nu * s;
+  }
+  T uf[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) uf[c] = T(0.5) * (ua[c] + ub[c]);
+  T ta = pa / (ra * K<T>::r_gas());
+  T tb = pb / (rb * K<T>::r_gas());
+  T ka = inv_pr * K<T>::cp() * (nu * ra);
+  T kb = inv_pr * K<T>::cp() * (nu * rb);
+  T q = -(T(0.5) * (ka + kb)) * ((tb - ta) / h_d);
+  T dot = uf[0] * tau[0] + uf[1] * tau[1] + uf[2] * tau[2];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) f[1 + c] = f[1 + c] + (-tau[c]);
+  f[4] = f[4] + (q + (-dot));
+}
+
+}  // namespace swc

@@ -1,0 +1,88 @@
+// Instantiates the fused stage kernel for one (dtype, scheme) pair; compiled
+// once per pair with -DSWC_T=<float|double> -DSWC_SCHEME=<0..3>
+// -DSWC_SUFFIX=<name> so the 32 kernel variants build in parallel.
+#include "swc_launch.h"
+
+#ifndef SWC_T
+#error "SWC_T must be defined"
+#endif
+
+#ifndef SWC_MULTI_TILE
+#define SWC_MULTI_TILE 0
+#endif
+
+#define SWC_CAT2(a, b) a##b
+#define SWC_CAT(a, b) SWC_CAT2(a, b)
+
+namespace swc {
+namespace {
+
+// Tile shapes (TY along y, TX along x); 256 threads each.
+template <typename T, int RM, bool V, int TY, int TX>
+int launch_tile(const StageArgs& a, cudaStream_t st) {
+  using Lay = Layout<T, SWC_SCHEME, V, TY, TX>;
+  auto kern = stage_kernel<T, SWC_SCHEME, RM, V, TY, TX>;
+  // Set once per process (before any graph capture: the first launch of a
+  // variant is always eager).
+  static int attr_set = 0;
+  cudaError_t e;
+  if (!attr_set) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Lay::SMEM);
+    if (e != cudaSuccess) return SWC_ERR_LAUNCH;
+    attr_set = 1;
+  }
+  dim3 grid((a.ny + TY - 1) / TY, (a.nx + TX - 1) / TX,
+            (a.nz + a.zseg - 1) / a.zseg);
+  kern<<<grid, TY * TX, Lay::SMEM, st>>>(a);
+  note_launch();
+  e = cudaGetLastError();
+  return e == cudaSuccess ? SWC_OK : SWC_ERR_LAUNCH;
+}
+
+template <typename T, int RM, bool V>
+int launch_rm(const StageArgs& a, int tile, cudaStream_t st) {
+#if SWC_MULTI_TILE
+  switch (tile) {
+    case 1: return launch_tile<T, RM, V, 16, 16>(a, st);
+    case 2: return launch_tile<T, RM, V, 8, 32>(a, st);
+    default: return launch_tile<T, RM, V, 32, 8>(a, st);
+  }
+#else
+  (void)tile;
+  return launch_tile<T, RM, V, 32, 8>(a, st);
+#endif
+}
+
+template <typename T, bool V>
+size_t smem_tile(int tile) {
+#if SWC_MULTI_TILE
+  switch (tile) {
+    case 1: return Layout<T, SWC_SCHEME, V, 16, 16>::SMEM;
+    case 2: return Layout<T, SWC_SCHEME, V, 8, 32>::SMEM;
+    default: return Layout<T, SWC_SCHEME, V, 32, 8>::SMEM;
+  }
+#else
+  (void)tile;
+  return Layout<T, SWC_SCHEME, V, 32, 8>::SMEM;
+#endif
+}
+
+}  // namespace
+
+int SWC_CAT(launch_stage_, SWC_SUFFIX)(const StageArgs& a, int riemann,
+                                       int visc, int tile, cudaStream_t st) {
+  using T = SWC_T;
+  if (riemann == SWC_HLL)
+    return visc ? launch_rm<T, 0, true>(a, tile, st)
+                : launch_rm<T, 0, false>(a, tile, st);
+  return visc ? launch_rm<T, 1, true>(a, tile, st)
+              : launch_rm<T, 1, false>(a, tile, st);
+}
+
+size_t SWC_CAT(stage_smem_, SWC_SUFFIX)(int visc, int tile) {
+  using T = SWC_T;
+  return visc ? smem_tile<T, true>(tile) : smem_tile<T, false>(tile);
+}
+
+}  // namespace swc

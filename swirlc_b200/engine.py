@@ -1,0 +1,385 @@
+"""Device-side domain description and the fused step loop.
+
+`Solver` turns a reference config (`SwirlCParameters`) plus the shape and
+dtype of one replica's fields into the C-ABI descriptors (SwcGrid, SwcScheme,
+SwcFieldBC) and issues the kernels of libswirlc_b200.so on the current torch
+CUDA stream. `Stepper` owns the work buffers and the device clock of a
+time loop and can capture one step in a CUDA graph.
+
+Fields are torch CUDA tensors in the reference layout [nz+2h, nx+2h, ny+2h]
+(y contiguous), halos included, ordered rho, rho_u, rho_v, rho_w, rho_e.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from swirlc_b200 import _native as nat
+from swirlc_b200.boundary import bc_types
+from swirlc_b200.common import types
+from swirlc_b200.common import utils
+from swirlc_b200.physics import constant
+
+_INTERP = {'WENO_5': nat.SWC_WENO5, 'WENO_3': nat.SWC_WENO3,
+           'MUSCL': nat.SWC_MUSCL, 'NODE': nat.SWC_NODE}
+_LIMITER = {'van_leer': nat.SWC_LIM_VAN_LEER, 'mc': nat.SWC_LIM_MC,
+            'minmod': nat.SWC_LIM_MINMOD}
+_CELL_AVG = bc_types.BoundaryDictionaryType.CELL_AVERAGES.value
+_CELL_FACE = bc_types.BoundaryDictionaryType.CELL_FACES.value
+_CELL_FLUX = bc_types.BoundaryDictionaryType.INTERCELL_FLUXES.value
+
+
+def interp_code(cfg) -> int:
+  """Scheme code; errors as compressible_navier_stokes.py:581-595."""
+  scheme = getattr(cfg, 'interpolation_scheme', None)
+  if scheme not in _INTERP:
+    raise NotImplementedError(
+        f'"{scheme}" is not implemented as an "interpolation_scheme". Valid '
+        "options are: ['WENO_3', 'WENO_5', 'MUSCL']")
+  return _INTERP[scheme]
+
+
+def riemann_code(cfg) -> int:
+  """Flux code; errors as riemann_solver.py:53-62."""
+  scheme = getattr(cfg, 'numeric_flux_scheme', None)
+  if scheme == 'HLL':
+    return nat.SWC_HLL
+  if scheme == 'HLLC':
+    return nat.SWC_HLLC
+  raise ValueError(
+      f'"{scheme}" is not implemented as a "numeric_flux_scheme". Valid '
+      "options are: ['HLL', 'HLLC']")
+
+
+def _plane(val, dim: int, shape3: Sequence[int], dtype, device) -> torch.Tensor:
+  """A Dirichlet layer value as a [A, B] plane (see SwcBC.planes)."""
+  nz, nx, ny = shape3
+  ab = {0: (nz, ny), 1: (nz, nx), 2: (nx, ny)}[dim]
+  if isinstance(val, (int, float, np.floating, np.integer)):
+    return torch.full(ab, float(val), dtype=dtype, device=device)
+  if isinstance(val, (list, tuple)):
+    t = torch.stack([torch.as_tensor(np.asarray(
+        v.cpu() if isinstance(v, torch.Tensor) else v)) for v in val])
+  else:
+    t = torch.as_tensor(np.asarray(val.cpu() if isinstance(val, torch.Tensor)
+                                   else val))
+  t = t.to(dtype=dtype).reshape(ab).to(device)
+  return t.contiguous()
+
+
+def fill_field_bc(fbc, spec, via: int, shape3, hw: int, dtype, device,
+                  name: str = '') -> list:
+  """Fills one SwcFieldBC from a reference per-variable BC dict
+  {dim: {0: (type, value), 1: (type, value)}} (bc_types.BCDict).
+
+  Returns the device tensors that back per-layer Dirichlet planes; keep them
+  alive while the descriptor is in use.
+  """
+  keep = []
+  fbc.via_primitive = via
+  for di, dim in enumerate(types.DIMS):
+    sides = spec.get(dim) if isinstance(spec, dict) else None
+    if not sides:
+      for s in range(2):
+        fbc.side[di][s].kind = nat.SWC_BC_NONE
+      continue
+    # A PERIODIC entry makes the dim periodic (boundary.py:65-68).
+    periodic = any(bc_types.bc_value(sides[s][0]) == 0 for s in (0, 1)
+                   if s in sides)
+    for s in range(2):
+      b = fbc.side[di][s]
+      if periodic:
+        b.kind = nat.SWC_BC_PERIODIC
+        continue
+      kind = bc_types.bc_value(sides[s][0])
+      val = sides[s][1] if len(sides[s]) > 1 else 0.0
+      if kind == bc_types.BoundaryCondition.DIRICHLET.value:
+        b.kind = nat.SWC_BC_DIRICHLET
+        if isinstance(val, (list, tuple)):
+          layers = [_plane(v, di, shape3, dtype, device) for v in val]
+          if len(layers) != hw:
+            raise ValueError(
+                f'Dirichlet BC for {name} along {dim} has {len(layers)} '
+                f'layers; halo_width is {hw}.')
+          planes = torch.stack(layers).contiguous()
+          keep.append(planes)
+          b.per_layer = 1
+          b.planes = planes.data_ptr()
+        elif isinstance(val, (torch.Tensor, np.ndarray)) and np.ndim(val) > 0:
+          pl = _plane(val, di, shape3, dtype, device)
+          planes = pl.unsqueeze(0).expand(hw, *pl.shape).contiguous()
+          keep.append(planes)
+          b.per_layer = 1
+          b.planes = planes.data_ptr()
+        else:
+          b.value = float(val)
+      elif kind == bc_types.BoundaryCondition.NEUMANN.value:
+        if np.ndim(val) != 0:
+          raise NotImplementedError('Only scalar Neumann values are supported.')
+        b.kind = nat.SWC_BC_NEUMANN
+        b.value = float(val)
+      else:
+        raise NotImplementedError(f'Unsupported BC type {sides[s][0]}.')
+  return keep
+
+
+class Solver:
+  """One replica's grid, scheme and boundary conditions on the device."""
+
+  def __init__(self, cfg, physics_models, shape: Sequence[int],
+               dtype: torch.dtype = torch.float32,
+               device: Optional[torch.device] = None, replica_id: int = 0,
+               replicas: Optional[np.ndarray] = None,
+               names: Optional[Sequence[str]] = None,
+               interp_override: Optional[str] = None):
+    nat.load()
+    self.cfg = cfg
+    self.pm = physics_models
+    self.dtype = dtype
+    self.device = device or torch.device('cuda', torch.cuda.current_device())
+    self.names = list(names or cfg.conservative_variable_names)
+    if self.names[:5] != list(types.BASE_CONSERVATIVE) or len(self.names) != 5:
+      extra = [n for n in self.names if n not in types.BASE_CONSERVATIVE]
+      if extra:
+        raise NotImplementedError(
+            f'Transported scalars {extra} are not supported by the fused '
+            'CUDA path yet.')
+      self.names = list(types.BASE_CONSERVATIVE)
+    hw = int(cfg.halo_width)
+    nza, nxa, nya = (int(s) for s in shape)
+    self.shape = (nza, nxa, nya)
+    self.hw = hw
+    self.nx, self.ny, self.nz = nxa - 2 * hw, nya - 2 * hw, nza - 2 * hw
+    if min(self.nx, self.ny, self.nz) <= 0:
+      raise ValueError(f'Field shape {shape} is too small for halo_width {hw}.')
+    self.grid = nat.SwcGrid(self.nx, self.ny, self.nz, hw, nya, nya * nxa,
+                            float(cfg.dx), float(cfg.dy), float(cfg.dz))
+    if _CELL_FACE in cfg.bc or _CELL_FLUX in cfg.bc:
+      raise NotImplementedError(
+          'Face and flux boundary conditions are not supported by the fused '
+          'CUDA path yet.')
+    sc = nat.SwcScheme()
+    sc.dtype = nat.dtype_code(dtype)
+    sc.interp = (_INTERP[interp_override] if interp_override
+                 else interp_code(cfg))
+    lim = getattr(cfg, 'muscl_limiter', 'van_leer')
+    if lim not in _LIMITER:
+      raise ValueError(f'Unknown MUSCL limiter "{lim}".')
+    sc.limiter = _LIMITER[lim]
+    sc.riemann = riemann_code(cfg)
+    sc.diffusion = 1 if cfg.include_diffusion else 0
+    sc.nscalars = 0
+    sc.gravity_mask = physics_models.gravity_mask()
+    sc.zseg = int(getattr(cfg, 'zseg', 0) or 0)
+    sc.tile = int(getattr(cfg, 'tile', 0) or 0)
+    sc.nu = physics_models.transport_model.nu
+    sc.pr = physics_models.transport_model.pr
+    for i, d in enumerate(types.DIMS):
+      sc.g[i] = float(cfg.g[d])
+    self._pe = [None, None, None]
+    if utils.gravity_direction(cfg) != -1:
+      reps = replicas if replicas is not None else np.array([[[0]]])
+      mesh = utils.mesh_local(replica_id, reps, cfg)
+      for i, d in enumerate(types.DIMS):
+        coef = constant.G * float(cfg.g[d])
+        if coef != 0.0:
+          a = torch.as_tensor(coef * mesh[d].astype(np.float64), dtype=dtype)
+          n_expect = {0: nxa, 1: nya, 2: nza}[i]
+          if a.numel() != n_expect:
+            raise ValueError(
+                f'Mesh along {d} has {a.numel()} points with halos; the '
+                f'fields have {n_expect}.')
+          self._pe[i] = a.to(self.device).contiguous()
+          sc.pe_axis[i] = self._pe[i].data_ptr()
+    self.scheme = sc
+    self._build_bcs()
+    self._dt_cache: Dict[float, torch.Tensor] = {}
+
+  # ------------------------------------------------------------------ BCs
+  def _build_bcs(self):
+    bc_all = self.cfg.bc.get(_CELL_AVG, {})
+    self._planes = []
+    arr = (nat.SwcFieldBC * len(self.names))()
+    for fi, name in enumerate(self.names):
+      prim_name = types.conservative_to_primitive_name(name)
+      if name in bc_all:
+        spec, via = bc_all[name], 0
+      elif prim_name in bc_all:
+        spec, via = bc_all[prim_name], 1
+      else:
+        raise ValueError(
+            'A "cells" boundary condition is required for all conservative'
+            ' variables, either directly or through their respective'
+            f' primitive. No boundary condition was found for {name} or'
+            f' {prim_name}.')
+      self._planes += fill_field_bc(arr[fi], spec, via, self.shape, self.hw,
+                                    self.dtype, self.device, name)
+    self.bcs = arr
+
+  # -------------------------------------------------------------- kernels
+  def check_fields(self, fields: Sequence[torch.Tensor]) -> None:
+    if len(fields) != 5:
+      raise ValueError('Expected 5 conserved fields.')
+    for f in fields:
+      if (tuple(f.shape) != self.shape or f.dtype != self.dtype or
+          not f.is_cuda or not f.is_contiguous()):
+        raise ValueError(
+            f'Field of shape {tuple(f.shape)} / {f.dtype} does not match the '
+            f'solver ({self.shape}, {self.dtype}, contiguous CUDA).')
+
+  def dt_tensor(self, dt: float) -> torch.Tensor:
+    t = self._dt_cache.get(dt)
+    if t is None:
+      t = torch.tensor([float(dt)], dtype=torch.float64, device=self.device)
+      self._dt_cache[dt] = t
+    return t
+
+  def fill_halos(self, fields: Sequence[torch.Tensor]) -> None:
+    """In-place halo fill (boundary.update_conservative_cell_averages)."""
+    ptrs = nat.ptr_array(fields)
+    nat.check(nat.load().swc_halo_fill(
+        ctypes.byref(self.grid), self.scheme.dtype, len(fields), ptrs,
+        self.bcs, 0, nat.stream_ptr()), 'halo fill')
+
+  def stage(self, uk, u0, uout, mode: int, c0: float = 0.0, c1: float = 0.0,
+            dt: Optional[torch.Tensor] = None,
+            dtmin_out: Optional[torch.Tensor] = None) -> None:
+    nat.check(nat.load().swc_rk_stage(
+        ctypes.byref(self.grid), ctypes.byref(self.scheme),
+        nat.ptr_array(uk), nat.ptr_array(u0) if u0 is not None else None,
+        nat.ptr_array(uout), mode, float(c0), float(c1),
+        dt.data_ptr() if dt is not None else None,
+        dtmin_out.data_ptr() if dtmin_out is not None else None,
+        nat.stream_ptr()), 'rk stage')
+
+  def cfl_reduce(self, fields, dtmin_out: torch.Tensor) -> None:
+    nat.check(nat.load().swc_cfl_reduce(
+        ctypes.byref(self.grid), ctypes.byref(self.scheme),
+        nat.ptr_array(fields), dtmin_out.data_ptr(), nat.stream_ptr()),
+        'cfl reduce')
+
+  def new_fields(self, zero: bool = True) -> List[torch.Tensor]:
+    alloc = torch.zeros if zero else torch.empty
+    return [alloc(self.shape, dtype=self.dtype, device=self.device)
+            for _ in range(5)]
+
+  def rhs(self, fields: Sequence[torch.Tensor]) -> List[torch.Tensor]:
+    """Functional RHS: copies, fills halos of the copy, returns dU/dt."""
+    work = [f.clone() for f in fields]
+    self.fill_halos(work)
+    out = self.new_fields(zero=True)
+    self.stage(work, None, out, nat.SWC_OUT_RHS)
+    return out
+
+  def rk3(self, fields: Sequence[torch.Tensor], dt: float) -> List[torch.Tensor]:
+    """Functional SSP-RK3 step (rk3.py:87-120) returning new fields."""
+    dtt = self.dt_tensor(dt)
+    u0 = [f.clone() for f in fields]
+    self.fill_halos(u0)
+    u1 = self.new_fields(zero=False)
+    self.stage(u0, None, u1, nat.SWC_OUT_EULER, dt=dtt)
+    self.fill_halos(u1)
+    u2 = self.new_fields(zero=False)
+    self.stage(u1, u0, u2, nat.SWC_OUT_CONVEX, 0.75, 0.25, dt=dtt)
+    self.fill_halos(u2)
+    self.stage(u2, u0, u1, nat.SWC_OUT_CONVEX, 1.0 / 3.0, 2.0 / 3.0, dt=dtt)
+    self.fill_halos(u1)
+    return u1
+
+  def rk2(self, fields: Sequence[torch.Tensor], dt: float) -> List[torch.Tensor]:
+    """Functional RK2 step (rk2.py:63-86) returning new fields."""
+    dtt = self.dt_tensor(dt)
+    u0 = [f.clone() for f in fields]
+    self.fill_halos(u0)
+    u1 = self.new_fields(zero=False)
+    self.stage(u0, None, u1, nat.SWC_OUT_EULER, dt=dtt)
+    self.fill_halos(u1)
+    u2 = self.new_fields(zero=False)
+    self.stage(u1, u0, u2, nat.SWC_OUT_AVERAGE, 0.5, 0.0, dt=dtt)
+    self.fill_halos(u2)
+    return u2
+
+
+class Stepper:
+  """In-place time loop over a state with a device clock (no host syncs).
+
+  Each step: [clock begin] -> fill(u) -> stage EULER u->w1 -> fill(w1) ->
+  stage CONVEX (u, w1)->w2 -> fill(w2) -> stage CONVEX (u, w2)->u with the
+  fused CFL reduction -> [clock end]. With `cfl` > 0 the step size is
+  cfl * min(delta/(|u|+c)) computed on the device.
+  """
+
+  def __init__(self, solver: Solver, fields: Sequence[torch.Tensor],
+               dt: float = 0.0, cfl: float = 0.0, t_end: float = 0.0,
+               scheme: str = 'rk3'):
+    solver.check_fields(fields)
+    self.s = solver
+    self.u = list(fields)
+    self.w1 = solver.new_fields(zero=False)
+    self.w2 = solver.new_fields(zero=False)
+    self.scheme = scheme
+    if scheme not in ('rk3', 'rk2'):
+      raise NotImplementedError(f'"{scheme}" is not implemented as an '
+                                '"time_integration_scheme".')
+    # SwcClock: t, dt, dtmin, cfl, t_end, step (int64 bits in slot 5).
+    self.clock = torch.zeros(6, dtype=torch.float64, device=solver.device)
+    self.clock[1] = float(dt)
+    self.clock[2] = 1e300
+    self.clock[3] = float(cfl)
+    self.clock[4] = float(t_end)
+    self.cfl = float(cfl)
+    if self.cfl > 0.0:
+      solver.cfl_reduce(self.u, self.clock[2:3])
+    self.graph: Optional[torch.cuda.CUDAGraph] = None
+
+  @property
+  def dt_ptr(self) -> torch.Tensor:
+    return self.clock[1:2]
+
+  def _launch_step(self):
+    s, lib = self.s, nat.load()
+    st = nat.stream_ptr()
+    cptr = self.clock.data_ptr()
+    if self.cfl > 0.0:
+      nat.check(lib.swc_clock_begin_step(cptr, st), 'clock')
+    dt = self.clock[1:2]
+    dtmin = self.clock[2:3] if self.cfl > 0.0 else None
+    s.fill_halos(self.u)
+    s.stage(self.u, None, self.w1, nat.SWC_OUT_EULER, dt=dt)
+    s.fill_halos(self.w1)
+    if self.scheme == 'rk3':
+      s.stage(self.w1, self.u, self.w2, nat.SWC_OUT_CONVEX, 0.75, 0.25, dt=dt)
+      s.fill_halos(self.w2)
+      s.stage(self.w2, self.u, self.u, nat.SWC_OUT_CONVEX, 1.0 / 3.0,
+              2.0 / 3.0, dt=dt, dtmin_out=dtmin)
+    else:
+      s.stage(self.w1, self.u, self.u, nat.SWC_OUT_AVERAGE, 0.5, 0.0, dt=dt,
+              dtmin_out=dtmin)
+    nat.check(lib.swc_clock_end_step(cptr, st), 'clock')
+
+  def capture(self) -> None:
+    """Captures one step in a CUDA graph (after one eager warm-up step)."""
+    self.graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+      with torch.cuda.graph(self.graph, stream=side):
+        self._launch_step()
+    torch.cuda.current_stream().wait_stream(side)
+
+  def step(self, n: int = 1) -> None:
+    for _ in range(n):
+      if self.graph is not None:
+        self.graph.replay()
+      else:
+        self._launch_step()
+
+  def time(self) -> float:
+    return float(self.clock[0].item())
+
+  def steps_done(self) -> int:
+    return int(self.clock[5:6].view(torch.int64).item())

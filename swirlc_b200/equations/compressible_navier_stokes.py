@@ -1,0 +1,100 @@
+"""Compressible Navier-Stokes RHS (reference: equations/compressible_navier_stokes.py).
+
+`get_rhs_fn(replicas, cfg, physics_models)` returns
+`rhs(replica_id, conservative, helper_vars) -> dict`, the same contract as
+compressible_navier_stokes.py:46-270: the conservative dict is copied, its
+halos filled from `cfg.bc`, and the time derivative of every conserved
+variable is returned (valid on interior cells; halo cells are zero). The
+whole chain of steps 1-9 (compressible_navier_stokes.py:99-267) runs as one
+fused CUDA stage kernel per call (swirlc_b200/csrc/swc_stage.cuh).
+"""
+
+import enum
+from typing import Dict
+
+import numpy as np
+import torch
+
+from swirlc_b200 import engine
+from swirlc_b200.boundary import bc_types
+from swirlc_b200.common import types
+from swirlc_b200.common import utils
+
+_CELL_FACE_BC = bc_types.BoundaryDictionaryType.CELL_FACES.value
+
+
+class InterpolationSchemes(enum.Enum):
+  """compressible_navier_stokes.py:39-43."""
+  WENO_3 = 'WENO_3'
+  WENO_5 = 'WENO_5'
+  MUSCL = 'MUSCL'
+
+
+class _SolverCache:
+  """Solvers keyed by field shape, dtype and device for one cfg."""
+
+  def __init__(self, replicas, cfg, physics_models, interp_override=None):
+    self.replicas = replicas
+    self.cfg = cfg
+    self.pm = physics_models
+    self.interp_override = interp_override
+    self._cache = {}
+
+  def get(self, replica_id, fields) -> engine.Solver:
+    f = fields[0]
+    key = (tuple(f.shape), f.dtype, f.device, int(replica_id))
+    s = self._cache.get(key)
+    if s is None:
+      s = engine.Solver(self.cfg, self.pm, f.shape, f.dtype, f.device,
+                        replica_id=int(replica_id), replicas=self.replicas,
+                        interp_override=self.interp_override)
+      self._cache[key] = s
+    return s
+
+
+def _check_cfg(cfg):
+  engine.interp_code(cfg)
+  engine.riemann_code(cfg)
+  if cfg.include_diffusion and _CELL_FACE_BC in cfg.bc:
+    raise NotImplementedError(
+        'Face boundary conditions are not supported with diffusion enabled at'
+        ' this time.')
+
+
+def _ordered_fields(conservative) -> list:
+  missing = [n for n in types.BASE_CONSERVATIVE if n not in conservative]
+  if missing:
+    raise ValueError(f'Missing conservative variables {missing}.')
+  extra = [n for n in conservative if n not in types.BASE_CONSERVATIVE]
+  if extra:
+    raise NotImplementedError(
+        f'Transported scalars {extra} are not supported by the fused CUDA '
+        'path yet.')
+  out = []
+  for n in types.BASE_CONSERVATIVE:
+    t = utils.as_tensor3d(conservative[n])
+    if not t.is_cuda:
+      raise ValueError(f'Field {n} must be a CUDA tensor.')
+    out.append(t.contiguous())
+  return out
+
+
+def get_rhs_fn(replicas: np.ndarray, cfg, physics_models):
+  """compressible_navier_stokes.py:46-270."""
+  _check_cfg(cfg)
+  cache = _SolverCache(replicas, cfg, physics_models,
+                       getattr(cfg, '_interp_override', None))
+
+  def rhs(replica_id, conservative: Dict, helper_vars: Dict) -> Dict:
+    if helper_vars and ('p_ref' in helper_vars or 'rho_ref' in helper_vars):
+      raise NotImplementedError(
+          'Helper reference states (p_ref, rho_ref) are not supported by the '
+          'fused CUDA path yet.')
+    fields = _ordered_fields(conservative)
+    solver = cache.get(replica_id, fields)
+    out = solver.rhs(fields)
+    res = dict(zip(types.BASE_CONSERVATIVE, out))
+    return {k: utils.like_input(res[k], conservative[k]) for k in conservative}
+
+  rhs._swc_cache = cache  # lets rk3/rk2 run the fused in-place stages
+  return rhs

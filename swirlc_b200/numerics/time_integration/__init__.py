@@ -1,0 +1,1 @@
+"""swirlc_b200 subpackage mirroring the reference module of the same name."""
