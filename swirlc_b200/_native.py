@@ -14,8 +14,10 @@ from typing import Optional, Sequence
 
 import torch
 
-_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'lib',
-                         'libswirlc_b200.so')
+# SWIRLC_B200_LIB overrides the in-tree library path (e.g. an alternative
+# build of the same sources).
+_LIB_PATH = os.environ.get('SWIRLC_B200_LIB') or os.path.join(
+    os.path.dirname(os.path.abspath(__file__)), 'lib', 'libswirlc_b200.so')
 
 SWC_OK = 0
 SWC_ERR_ARG = -1

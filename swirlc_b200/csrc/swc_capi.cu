@@ -491,7 +491,7 @@ int swc_rk_stage(const SwcGrid* grid, const SwcScheme* sc,
   // z segment per CTA: enough CTAs for ~4 waves of 2 CTAs/SM, >= 8 planes.
   int zseg = sc->zseg;
   if (zseg <= 0) {
-    long long tiles2d = (long long)((grid->ny + 31) / 32) * ((grid->nx + 7) / 8);
+    long long tiles2d = (long long)((grid->ny + 15) / 16) * ((grid->nx + 15) / 16);
     long long nseg = std::max<long long>(1, (148 * 2 * 4 + tiles2d - 1) / tiles2d);
     zseg = (int)std::max<long long>(8, (grid->nz + nseg - 1) / nseg);
   }

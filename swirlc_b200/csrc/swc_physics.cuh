@@ -8,6 +8,13 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// 1: single-precision WENO runs the neg/pos pair as f32x2 instructions
+// (measured slower on B200: operand-pair moves outweigh the halved FP32
+// issue count, so the scalar form is the default).
+#ifndef SWC_PACKED_WENO
+#define SWC_PACKED_WENO 0
+#endif
+
 namespace swc {
 
 // physics/constant.py:17-41. Python doubles rounded once to T, as TF does
@@ -185,15 +192,100 @@ __device__ __forceinline__ T muscl_slope(T vm1, T v0, T vp1, int limiter) {
   return phi * dp;
 }
 
+// ---------------------------------------------------------------------------
+// Packed single-precision reconstruction. The neg value of face i-1/2 (right
+// face of cell i-1) and its pos value (left face of cell i) use the same
+// formulas on stencils shifted by one cell, with mirrored coefficients, so
+// both run as one sequence of Blackwell f32x2 instructions (FFMA2 / FADD2 /
+// FMUL2): lane x = neg, lane y = pos.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  return __ffma2_rn(a, b, c);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 rcp2(float2 a) {
+  return make_float2(1.0f / a.x, 1.0f / a.y);
+}
+
+// WENO5-JS pair from the 6-cell stencil s[0..5] = v[i-3..i+2].
+__device__ __forceinline__ float2 weno5_pair(const float* s) {
+  const float2 vm2 = f2(s[0], s[1]), vm1 = f2(s[1], s[2]), v0 = f2(s[2], s[3]);
+  const float2 vp1 = f2(s[3], s[4]), vp2 = f2(s[4], s[5]);
+  const float2 k1312 = f2(13.0f / 12.0f, 13.0f / 12.0f);
+  const float2 kq = f2(0.25f, 0.25f), eps = f2(1e-6f, 1e-6f);
+  const float2 m2 = f2(-2.0f, -2.0f), k3 = f2(3.0f, 3.0f), m4 = f2(-4.0f, -4.0f);
+  // beta_0 on (v0, vp1, vp2)
+  float2 a = add2(fma2(m2, vp1, v0), vp2);
+  float2 b = fma2(m4, vp1, fma2(k3, v0, vp2));
+  float2 b0 = fma2(mul2(k1312, a), a, mul2(mul2(kq, b), b));
+  // beta_1 on (vm1, v0, vp1)
+  a = add2(fma2(m2, v0, vm1), vp1);
+  b = add2(vm1, mul2(f2(-1.0f, -1.0f), vp1));
+  float2 b1 = fma2(mul2(k1312, a), a, mul2(mul2(kq, b), b));
+  // beta_2 on (vm2, vm1, v0)
+  a = add2(fma2(m2, vm1, vm2), v0);
+  b = fma2(k3, v0, fma2(m4, vm1, vm2));
+  float2 b2 = fma2(mul2(k1312, a), a, mul2(mul2(kq, b), b));
+  b0 = add2(b0, eps);
+  b1 = add2(b1, eps);
+  b2 = add2(b2, eps);
+  // alpha_r = d_r / (eps + beta_r)^2; d = (0.3, 0.6, 0.1) for neg and the
+  // mirror (0.1, 0.6, 0.3) for pos.
+  const float2 a0 = mul2(f2(0.3f, 0.1f), rcp2(mul2(b0, b0)));
+  const float2 a1 = mul2(f2(0.6f, 0.6f), rcp2(mul2(b1, b1)));
+  const float2 a2 = mul2(f2(0.1f, 0.3f), rcp2(mul2(b2, b2)));
+  // Candidates: neg = right face of the cell, pos = left face.
+  const float2 q0 = fma2(f2(-1.0f / 6.0f, 1.0f / 3.0f), vp2,
+                         fma2(f2(5.0f / 6.0f, -7.0f / 6.0f), vp1,
+                              mul2(f2(1.0f / 3.0f, 11.0f / 6.0f), v0)));
+  const float2 q1 = fma2(f2(1.0f / 3.0f, -1.0f / 6.0f), vp1,
+                         fma2(f2(5.0f / 6.0f, 5.0f / 6.0f), v0,
+                              mul2(f2(-1.0f / 6.0f, 1.0f / 3.0f), vm1)));
+  const float2 q2 = fma2(f2(11.0f / 6.0f, 1.0f / 3.0f), v0,
+                         fma2(f2(-7.0f / 6.0f, 5.0f / 6.0f), vm1,
+                              mul2(f2(1.0f / 3.0f, -1.0f / 6.0f), vm2)));
+  const float2 num = fma2(a2, q2, fma2(a1, q1, mul2(a0, q0)));
+  const float2 den = add2(add2(a0, a1), a2);
+  return mul2(num, rcp2(den));
+}
+
+// WENO3-JS pair from s[0..3] = v[i-2..i+1].
+__device__ __forceinline__ float2 weno3_pair(const float* s) {
+  const float2 vm1 = f2(s[0], s[1]), v0 = f2(s[1], s[2]), vp1 = f2(s[2], s[3]);
+  const float2 eps = f2(1e-6f, 1e-6f);
+  float2 d0 = add2(vp1, mul2(f2(-1.0f, -1.0f), v0));
+  float2 d1 = add2(v0, mul2(f2(-1.0f, -1.0f), vm1));
+  float2 b0 = fma2(d0, d0, eps), b1 = fma2(d1, d1, eps);
+  const float2 a0 = mul2(f2(2.0f / 3.0f, 1.0f / 3.0f), rcp2(mul2(b0, b0)));
+  const float2 a1 = mul2(f2(1.0f / 3.0f, 2.0f / 3.0f), rcp2(mul2(b1, b1)));
+  const float2 q0 = fma2(f2(0.5f, -0.5f), vp1, mul2(f2(0.5f, 1.5f), v0));
+  const float2 q1 = fma2(f2(1.5f, 0.5f), v0, mul2(f2(-0.5f, 0.5f), vm1));
+  return mul2(fma2(a1, q1, mul2(a0, q0)), rcp2(add2(a0, a1)));
+}
+
 template <int SCHEME, typename T>
 __device__ __forceinline__ void reconstruct(const T* s, int limiter, T& neg,
                                             T& pos) {
   if constexpr (SCHEME == 0) {
-    neg = weno5_right(s[0], s[1], s[2], s[3], s[4]);
-    pos = weno5_left(s[1], s[2], s[3], s[4], s[5]);
+    if constexpr (sizeof(T) == 4 && SWC_PACKED_WENO) {
+      float2 r = weno5_pair(s);
+      neg = r.x;
+      pos = r.y;
+    } else {
+      neg = weno5_right(s[0], s[1], s[2], s[3], s[4]);
+      pos = weno5_left(s[1], s[2], s[3], s[4], s[5]);
+    }
   } else if constexpr (SCHEME == 1) {
-    neg = weno3_right(s[0], s[1], s[2]);
-    pos = weno3_left(s[1], s[2], s[3]);
+    if constexpr (sizeof(T) == 4 && SWC_PACKED_WENO) {
+      float2 r = weno3_pair(s);
+      neg = r.x;
+      pos = r.y;
+    } else {
+      neg = weno3_right(s[0], s[1], s[2]);
+      pos = weno3_left(s[1], s[2], s[3]);
+    }
   } else if constexpr (SCHEME == 2) {
     neg = s[1] + T(0.5) * muscl_slope(s[0], s[1], s[2], limiter);
     pos = s[2] - T(0.5) * muscl_slope(s[1], s[2], s[3], limiter);

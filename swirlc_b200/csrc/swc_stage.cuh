@@ -81,12 +81,36 @@ struct Layout {
   static constexpr int PH = TX + 2 * G::HR;
   static constexpr int PS = PW * PH;
   static constexpr int NT = TX * TY;
+  static constexpr int PER = (PS + NT - 1) / NT;  // plane cells per thread
   static constexpr int RING_ELEMS = G::RING * 7 * PS;
+  static constexpr int STAGE_ELEMS = 5 * PS;
   static constexpr int FY_ELEMS = 5 * TX * (TY + 1);
   static constexpr int FX_ELEMS = 5 * (TX + 1) * TY;
+  static constexpr int FZ_ELEMS = 5 * TX * TY;
   static constexpr size_t SMEM =
-      sizeof(T) * (size_t)(RING_ELEMS + FY_ELEMS + FX_ELEMS);
+      sizeof(T) * (size_t)(RING_ELEMS + STAGE_ELEMS + FY_ELEMS + FX_ELEMS +
+                           FZ_ELEMS);
 };
+
+// 4- or 8-byte asynchronous global->shared copy (LDGSTS), cached in L1 so
+// the centre-plane reload of the stage update hits on chip.
+template <typename T>
+__device__ __forceinline__ void cp_async(T* smem, const T* gmem) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  if constexpr (sizeof(T) == 4) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s),
+                 "l"(gmem));
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s),
+                 "l"(gmem));
+  }
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
 
 template <typename T, int SCHEME, int RIEMANN, bool VISC, int TY, int TX>
 __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
@@ -95,12 +119,14 @@ __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
   using L = Layout<T, SCHEME, VISC, TY, TX>;
   constexpr int LO = G::LO, NW = G::NW, HR = G::HR, ZLO = G::ZLO,
                 ZHI = G::ZHI, RING = G::RING;
-  constexpr int PW = L::PW, PH = L::PH, PS = L::PS, NT = L::NT;
+  constexpr int PW = L::PW, PH = L::PH, PS = L::PS, NT = L::NT, PER = L::PER;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* ring = reinterpret_cast<T*>(smem_raw);
-  T* fy = ring + L::RING_ELEMS;  // [5][TX][TY+1]
-  T* fx = fy + L::FY_ELEMS;      // [5][TX+1][TY]
+  T* stg = ring + L::RING_ELEMS;  // [5][PS] conserved plane in flight
+  T* fy = stg + L::STAGE_ELEMS;   // [5][TX][TY+1]
+  T* fx = fy + L::FY_ELEMS;       // [5][TX+1][TY]
+  T* fz = fx + L::FX_ELEMS;       // [5][TX][TY]
 
   const int tid = threadIdx.x;
   const int ty = tid % TY, tx = tid / TY;
@@ -111,11 +137,9 @@ __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
   const int nxa = a.nx + 2 * h, nya = a.ny + 2 * h;
   const long long sx = a.sx, sz = a.sz;
 
-  const T* __restrict__ uk0 = static_cast<const T*>(a.uk[0]);
-  const T* __restrict__ uk1 = static_cast<const T*>(a.uk[1]);
-  const T* __restrict__ uk2 = static_cast<const T*>(a.uk[2]);
-  const T* __restrict__ uk3 = static_cast<const T*>(a.uk[3]);
-  const T* __restrict__ uk4 = static_cast<const T*>(a.uk[4]);
+  const T* __restrict__ ukp[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) ukp[v] = static_cast<const T*>(a.uk[v]);
   const T* __restrict__ pex = static_cast<const T*>(a.pe[0]);
   const T* __restrict__ pey = static_cast<const T*>(a.pe[1]);
   const T* __restrict__ pez = static_cast<const T*>(a.pe[2]);
@@ -134,26 +158,47 @@ __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
   auto R = [&](int slot, int v, int px, int py) -> T& {
     return ring[((slot * 7 + v) * PH + px) * PW + py];
   };
-  auto load_plane = [&](int z, int slot) {
-    const int za = z + h;
-    for (int idx = tid; idx < PS; idx += NT) {
-      int px = idx / PW, py = idx - px * PW;
-      int xa = x0 - HR + px + h, ya = y0 - HR + py + h;
-      T r = T(1), ru = T(0), rv = T(0), rw = T(0), re = T(1), pe = T(0);
-      if (xa < nxa && ya < nya) {
-        long long o = za * sz + xa * sx + ya;
-        r = __ldg(uk0 + o);
-        ru = __ldg(uk1 + o);
-        rv = __ldg(uk2 + o);
-        rw = __ldg(uk3 + o);
-        re = __ldg(uk4 + o);
-        pe = pe_at(xa, ya, za);
+  // Plane cells this thread stages and converts: idx = tid + k*NT.
+  auto cell_valid = [&](int idx, int& xa, int& ya) -> bool {
+    const int px = idx / PW, py = idx - px * PW;
+    xa = x0 - HR + px + h;
+    ya = y0 - HR + py + h;
+    return idx < PS && xa < nxa && ya < nya;
+  };
+  auto issue_plane = [&](int z) {
+    const long long zo = (long long)(z + h) * sz;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int idx = tid + k * NT;
+      int xa, ya;
+      if (cell_valid(idx, xa, ya)) {
+        const long long o = zo + xa * sx + ya;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) cp_async(stg + v * PS + idx, ukp[v] + o);
       }
-      T u, v, w, e, p, hh;
-      cons_to_prim(r, ru, rv, rw, re, pe, u, v, w, e, p, hh);
-      R(slot, 0, px, py) = r;
+    }
+    cp_async_commit();
+  };
+  // Converts this thread's staged cells into ring slot `slot` (plane z).
+  auto convert_plane = [&](int z, int slot) {
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int idx = tid + k * NT;
+      if (idx >= PS) break;
+      int xa, ya;
+      T c[5] = {T(1), T(0), T(0), T(0), T(1)};
+      T pe = T(0);
+      if (cell_valid(idx, xa, ya)) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) c[v] = stg[v * PS + idx];
+        pe = pe_at(xa, ya, z + h);
+      }
+      T u, vv, w, e, p, hh;
+      cons_to_prim(c[0], c[1], c[2], c[3], c[4], pe, u, vv, w, e, p, hh);
+      const int px = idx / PW, py = idx - px * PW;
+      R(slot, 0, px, py) = c[0];
       R(slot, 1, px, py) = u;
-      R(slot, 2, px, py) = v;
+      R(slot, 2, px, py) = vv;
       R(slot, 3, px, py) = w;
       R(slot, 4, px, py) = e;
       R(slot, 5, px, py) = p;
@@ -163,167 +208,191 @@ __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
   const int zfirst = z0 - ZLO - 1;
   auto slot_of = [&](int z) { return (z - zfirst) % RING; };
 
-  // z-face above cell (tx, ty) of plane zc, i.e. face index zc + 1.
-  auto zface = [&](int zc, T* f) {
+  // ---- one face flux in the frame rotated so that the face normal is
+  // axis 0: (n, t1, t2) = x:(x,y,z), y:(y,x,z), z:(z,x,y). The same code
+  // serves all three face directions; only ring offsets differ.
+  //   off[k]   ring offset of stencil cell k (cells i-LO .. i+RI-1) of var 0
+  //   ta/tb    ring offsets of the t1-/t1+/t2-/t2+ neighbours of the cells
+  //            a = i-1 and b = i (viscous cross derivatives)
+  auto hsel = [&](int d) -> T { return d == 0 ? dx : (d == 1 ? dy : dz); };
+  auto face = [&](int dn, const int* off, const int* ta, const int* tb, T pe,
+                  T* f) {
+    const int t1 = dn == 0 ? 1 : 0, t2 = dn == 2 ? 1 : 2;
+    const int vel[3] = {1 + dn, 1 + t1, 1 + t2};
     Prim<T> ql, qr;
 #pragma unroll
     for (int v = 0; v < 7; ++v) {
+      int vv = v;
+      if (v >= 1 && v <= 3) vv = vel[v - 1];
+      const T* base = ring + vv * PS;
       T s[NW];
 #pragma unroll
-      for (int k = 0; k < NW; ++k)
-        s[k] = R(slot_of(zc + 1 - LO + k), v, HR + tx, HR + ty);
+      for (int k = 0; k < NW; ++k) s[k] = base[off[k]];
       T ng, ps;
       reconstruct<SCHEME>(s, a.limiter, ng, ps);
       set_var(ql, v, ng);
       set_var(qr, v, ps);
     }
-    T pe = pe_at(x0 + tx + h, y0 + ty + h, zc + 1 + h);
-    riemann<RIEMANN, T, 2>(ql, qr, pe, f);
+    T g[5];
+    riemann<RIEMANN, T, 0>(ql, qr, pe, g);
     if constexpr (VISC) {
-      const int sa = slot_of(zc), sb = slot_of(zc + 1);
-      const int px = HR + tx, py = HR + ty;
+      const int oa = off[LO - 1], ob = off[LO];
       T ua[3], ub[3], ga[3][3], gb[3][3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        ua[c] = R(sa, 1 + c, px, py);
-        ub[c] = R(sb, 1 + c, px, py);
+        ua[c] = ring[vel[c] * PS + oa];
+        ub[c] = ring[vel[c] * PS + ob];
       }
-      // tangential x (rows) and y (cols); components c == t and c == 2.
-      const T i2dx = T(2) * dx, i2dy = T(2) * dy;
-      ga[0][0] = (R(sa, 1, px + 1, py) - R(sa, 1, px - 1, py)) / i2dx;
-      gb[0][0] = (R(sb, 1, px + 1, py) - R(sb, 1, px - 1, py)) / i2dx;
-      ga[0][2] = (R(sa, 3, px + 1, py) - R(sa, 3, px - 1, py)) / i2dx;
-      gb[0][2] = (R(sb, 3, px + 1, py) - R(sb, 3, px - 1, py)) / i2dx;
-      ga[1][1] = (R(sa, 2, px, py + 1) - R(sa, 2, px, py - 1)) / i2dy;
-      gb[1][1] = (R(sb, 2, px, py + 1) - R(sb, 2, px, py - 1)) / i2dy;
-      ga[1][2] = (R(sa, 3, px, py + 1) - R(sa, 3, px, py - 1)) / i2dy;
-      gb[1][2] = (R(sb, 3, px, py + 1) - R(sb, 3, px, py - 1)) / i2dy;
-      viscous_flux<T, 2>(R(sa, 0, px, py), R(sb, 0, px, py), ua, ub,
-                         R(sa, 5, px, py), R(sb, 5, px, py), ga, gb, dz, nu,
-                         inv_pr, f);
+      const T i2t1 = T(2) * hsel(t1), i2t2 = T(2) * hsel(t2);
+      // Along t1: components t1 (rotated 1) and n (rotated 0).
+      ga[1][1] = (ring[vel[1] * PS + ta[1]] - ring[vel[1] * PS + ta[0]]) / i2t1;
+      gb[1][1] = (ring[vel[1] * PS + tb[1]] - ring[vel[1] * PS + tb[0]]) / i2t1;
+      ga[1][0] = (ring[vel[0] * PS + ta[1]] - ring[vel[0] * PS + ta[0]]) / i2t1;
+      gb[1][0] = (ring[vel[0] * PS + tb[1]] - ring[vel[0] * PS + tb[0]]) / i2t1;
+      // Along t2: components t2 (rotated 2) and n.
+      ga[2][2] = (ring[vel[2] * PS + ta[3]] - ring[vel[2] * PS + ta[2]]) / i2t2;
+      gb[2][2] = (ring[vel[2] * PS + tb[3]] - ring[vel[2] * PS + tb[2]]) / i2t2;
+      ga[2][0] = (ring[vel[0] * PS + ta[3]] - ring[vel[0] * PS + ta[2]]) / i2t2;
+      gb[2][0] = (ring[vel[0] * PS + tb[3]] - ring[vel[0] * PS + tb[2]]) / i2t2;
+      viscous_flux<T, 0>(ring[oa], ring[ob], ua, ub, ring[5 * PS + oa],
+                         ring[5 * PS + ob], ga, gb, hsel(dn), nu, inv_pr, g);
+    }
+    // Back to (x, y, z) momentum order.
+    f[0] = g[0];
+    f[1] = dn == 0 ? g[1] : g[2];
+    f[2] = dn == 1 ? g[1] : (dn == 0 ? g[2] : g[3]);
+    f[3] = dn == 2 ? g[1] : g[3];
+    f[4] = g[4];
+  };
+
+  const int SL = 7 * PS;  // ring slot stride
+  // Face of kind `kind` (0 = x-face at row fxx, 1 = y-face at column fyy,
+  // 2 = z-face above plane zc) into the flux buffers.
+  auto do_face = [&](int kind, int zc, int fxx, int fyy) {
+    int off[NW], ta[4], tb[4];
+    T pe;
+    T f[5];
+    if (kind == 2) {
+      const int pos = (HR + fxx) * PW + HR + fyy;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) off[k] = slot_of(zc + 1 - LO + k) * SL + pos;
+      const int oa = slot_of(zc) * SL + pos, ob = slot_of(zc + 1) * SL + pos;
+      ta[0] = oa - PW; ta[1] = oa + PW; ta[2] = oa - 1; ta[3] = oa + 1;
+      tb[0] = ob - PW; tb[1] = ob + PW; tb[2] = ob - 1; tb[3] = ob + 1;
+      pe = pe_at(x0 + fxx + h, y0 + fyy + h, zc + 1 + h);
+      face(2, off, ta, tb, pe, f);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) fz[(v * TX + fxx) * TY + fyy] = f[v];
+    } else {
+      const int cs = slot_of(zc) * SL;
+      const int dm = (slot_of(zc - 1) - slot_of(zc)) * SL;
+      const int dp = (slot_of(zc + 1) - slot_of(zc)) * SL;
+      const int pos = cs + (HR + fxx) * PW + HR + fyy;
+      const int st = kind == 0 ? PW : 1;     // normal stride
+      const int s1 = kind == 0 ? 1 : PW;     // t1 stride (y for x-faces, x for y-faces)
+#pragma unroll
+      for (int k = 0; k < NW; ++k) off[k] = pos + (k - LO) * st;
+      const int oa = pos - st, ob = pos;
+      ta[0] = oa - s1; ta[1] = oa + s1; ta[2] = oa + dm; ta[3] = oa + dp;
+      tb[0] = ob - s1; tb[1] = ob + s1; tb[2] = ob + dm; tb[3] = ob + dp;
+      pe = pe_at(x0 + fxx + h, y0 + fyy + h, zc + h);
+      face(kind, off, ta, tb, pe, f);
+      if (kind == 0) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) fx[(v * (TX + 1) + fxx) * TY + fyy] = f[v];
+      } else {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) fy[(v * TX + fxx) * (TY + 1) + fyy] = f[v];
+      }
     }
   };
 
-  // ---- warm-up: planes zfirst .. z0+ZHI-1 and the z-face below z0.
-  for (int i = 0; i < RING; ++i) load_plane(zfirst + i, i);
+  // ---- warm-up: planes zfirst .. z0+ZHI-1 through the staging buffer.
+  for (int i = 0; i < RING; ++i) {
+    issue_plane(zfirst + i);
+    cp_async_wait_all();
+    convert_plane(zfirst + i, i);
+  }
+  issue_plane(z0 + ZHI);  // first plane of the main loop, in flight
   __syncthreads();
   const bool own = (x0 + tx < a.nx) && (y0 + ty < a.ny);
-  T flo[5], fhi[5];
-  if (own) zface(z0 - 1, flo);
+  T flo[5];
+  if (own) {
+    do_face(2, z0 - 1, tx, ty);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) flo[v] = fz[(v * TX + tx) * TY + ty];
+  }
+  // The first loop iteration overwrites the slot of plane z0-ZLO-1, which the
+  // z-face above reads, and the z-flux buffer.
   __syncthreads();
 
   double dtmin_local = 1e300;
   const double dt_d = a.dt ? *a.dt : 0.0;
   const T dt = T(dt_d);
   const T c0 = T(a.c0), c1 = T(a.c1);
+  const int xa_c = x0 + tx + h, ya_c = y0 + ty + h;
+
+  // Per plane every owner computes three faces of its cell (z above, y and
+  // x below); the last warp also computes the tile's high x-row and high
+  // y-column faces (TX + TY of them); owners of the last interior cell of a
+  // partial tile add the face beyond it.
+  const int wb = tid - (NT - 32);
+  int nj = own ? 3 : 0;
+  int bkind = -1, bx = 0, by = 0;
+  if (wb >= 0 && wb < TY + TX) {
+    if (wb < TY) { bkind = 0; bx = TX; by = wb; }
+    else { bkind = 1; bx = wb - TY; by = TY; }
+    if (bkind == 0 && !(x0 + TX <= a.nx && y0 + by < a.ny)) bkind = -1;
+    if (bkind == 1 && !(y0 + TY <= a.ny && x0 + bx < a.nx)) bkind = -1;
+  }
+  const bool ex_x = own && (x0 + tx + 1 == a.nx) && (tx + 1 < TX);
+  const bool ex_y = own && (y0 + ty + 1 == a.ny) && (ty + 1 < TY);
 
   for (int zc = z0; zc < z1; ++zc) {
-    // Plane zc+ZHI replaces plane zc-ZLO-1, last read before the previous
-    // barrier.
-    load_plane(zc + ZHI, slot_of(zc + ZHI));
+    // The plane zc+ZHI (staged during the previous plane) replaces the slot
+    // of plane zc-ZLO-1, last read before the barrier that ended the
+    // previous iteration.
+    cp_async_wait_all();
+    convert_plane(zc + ZHI, slot_of(zc + ZHI));
     __syncthreads();
-    const int cs = slot_of(zc);
-    const int sm1 = slot_of(zc - 1), sp1 = slot_of(zc + 1);
-    (void)sm1;
-    (void)sp1;
+    if (zc + 1 < z1) issue_plane(zc + ZHI + 1);
 
-    // ---- y-faces of plane zc: (TY+1) per row.
-    for (int f = tid; f < TX * (TY + 1); f += NT) {
-      const int fxx = f / (TY + 1), fyy = f - fxx * (TY + 1);
-      if (x0 + fxx >= a.nx || y0 + fyy > a.ny) continue;
-      Prim<T> ql, qr;
-#pragma unroll
-      for (int v = 0; v < 7; ++v) {
-        T s[NW];
-#pragma unroll
-        for (int k = 0; k < NW; ++k) s[k] = R(cs, v, HR + fxx, HR + fyy - LO + k);
-        T ng, ps;
-        reconstruct<SCHEME>(s, a.limiter, ng, ps);
-        set_var(ql, v, ng);
-        set_var(qr, v, ps);
-      }
-      T ff[5];
-      T pe = pe_at(x0 + fxx + h, y0 + fyy + h, zc + h);
-      riemann<RIEMANN, T, 1>(ql, qr, pe, ff);
-      if constexpr (VISC) {
-        const int px = HR + fxx, pa = HR + fyy - 1, pb = HR + fyy;
-        T ua[3], ub[3], ga[3][3], gb[3][3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          ua[c] = R(cs, 1 + c, px, pa);
-          ub[c] = R(cs, 1 + c, px, pb);
+    const int ntot = nj + (bkind >= 0) + ex_x + ex_y;
+    for (int j = 0; j < ntot; ++j) {
+      int kind, fxx, fyy;
+      if (j < nj) {
+        kind = 2 - j;  // z, y, x
+        fxx = tx;
+        fyy = ty;
+      } else {
+        int e = j - nj;
+        if (bkind >= 0 && e == 0) {
+          kind = bkind; fxx = bx; fyy = by;
+        } else {
+          if (bkind >= 0) --e;
+          if (e == 0 && ex_x) { kind = 0; fxx = tx + 1; fyy = ty; }
+          else { kind = 1; fxx = tx; fyy = ty + 1; }
         }
-        const T i2dx = T(2) * dx, i2dz = T(2) * dz;
-        ga[0][0] = (R(cs, 1, px + 1, pa) - R(cs, 1, px - 1, pa)) / i2dx;
-        gb[0][0] = (R(cs, 1, px + 1, pb) - R(cs, 1, px - 1, pb)) / i2dx;
-        ga[0][1] = (R(cs, 2, px + 1, pa) - R(cs, 2, px - 1, pa)) / i2dx;
-        gb[0][1] = (R(cs, 2, px + 1, pb) - R(cs, 2, px - 1, pb)) / i2dx;
-        ga[2][2] = (R(sp1, 3, px, pa) - R(sm1, 3, px, pa)) / i2dz;
-        gb[2][2] = (R(sp1, 3, px, pb) - R(sm1, 3, px, pb)) / i2dz;
-        ga[2][1] = (R(sp1, 2, px, pa) - R(sm1, 2, px, pa)) / i2dz;
-        gb[2][1] = (R(sp1, 2, px, pb) - R(sm1, 2, px, pb)) / i2dz;
-        viscous_flux<T, 1>(R(cs, 0, px, pa), R(cs, 0, px, pb), ua, ub,
-                           R(cs, 5, px, pa), R(cs, 5, px, pb), ga, gb, dy, nu,
-                           inv_pr, ff);
       }
-#pragma unroll
-      for (int v = 0; v < 5; ++v) fy[(v * TX + fxx) * (TY + 1) + fyy] = ff[v];
+      do_face(kind, zc, fxx, fyy);
     }
-
-    // ---- x-faces of plane zc: (TX+1) rows of TY.
-    for (int f = tid; f < (TX + 1) * TY; f += NT) {
-      const int fxx = f / TY, fyy = f - fxx * TY;
-      if (x0 + fxx > a.nx || y0 + fyy >= a.ny) continue;
-      Prim<T> ql, qr;
-#pragma unroll
-      for (int v = 0; v < 7; ++v) {
-        T s[NW];
-#pragma unroll
-        for (int k = 0; k < NW; ++k) s[k] = R(cs, v, HR + fxx - LO + k, HR + fyy);
-        T ng, ps;
-        reconstruct<SCHEME>(s, a.limiter, ng, ps);
-        set_var(ql, v, ng);
-        set_var(qr, v, ps);
-      }
-      T ff[5];
-      T pe = pe_at(x0 + fxx + h, y0 + fyy + h, zc + h);
-      riemann<RIEMANN, T, 0>(ql, qr, pe, ff);
-      if constexpr (VISC) {
-        const int py = HR + fyy, pa = HR + fxx - 1, pb = HR + fxx;
-        T ua[3], ub[3], ga[3][3], gb[3][3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          ua[c] = R(cs, 1 + c, pa, py);
-          ub[c] = R(cs, 1 + c, pb, py);
-        }
-        const T i2dy = T(2) * dy, i2dz = T(2) * dz;
-        ga[1][1] = (R(cs, 2, pa, py + 1) - R(cs, 2, pa, py - 1)) / i2dy;
-        gb[1][1] = (R(cs, 2, pb, py + 1) - R(cs, 2, pb, py - 1)) / i2dy;
-        ga[1][0] = (R(cs, 1, pa, py + 1) - R(cs, 1, pa, py - 1)) / i2dy;
-        gb[1][0] = (R(cs, 1, pb, py + 1) - R(cs, 1, pb, py - 1)) / i2dy;
-        ga[2][2] = (R(sp1, 3, pa, py) - R(sm1, 3, pa, py)) / i2dz;
-        gb[2][2] = (R(sp1, 3, pb, py) - R(sm1, 3, pb, py)) / i2dz;
-        ga[2][0] = (R(sp1, 1, pa, py) - R(sm1, 1, pa, py)) / i2dz;
-        gb[2][0] = (R(sp1, 1, pb, py) - R(sm1, 1, pb, py)) / i2dz;
-        viscous_flux<T, 0>(R(cs, 0, pa, py), R(cs, 0, pb, py), ua, ub,
-                           R(cs, 5, pa, py), R(cs, 5, pb, py), ga, gb, dx, nu,
-                           inv_pr, ff);
-      }
-#pragma unroll
-      for (int v = 0; v < 5; ++v) fx[(v * (TX + 1) + fxx) * TY + fyy] = ff[v];
-    }
-
-    // ---- z-face above each owned column.
-    if (own) zface(zc, fhi);
     __syncthreads();
 
     // ---- divergence, source and stage combination.
     if (own) {
-      const int xa = x0 + tx + h, ya = y0 + ty + h, za = zc + h;
-      const long long o = za * sz + xa * sx + ya;
+      const int za = zc + h;
+      const long long o = za * sz + (long long)xa_c * sx + ya_c;
+      T ukc[5], u0c[5];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        ukc[v] = __ldg(ukp[v] + o);
+        u0c[v] = (a.mode >= SWC_OUT_CONVEX)
+                     ? __ldg(static_cast<const T*>(a.u0[v]) + o)
+                     : T(0);
+      }
       T src[5] = {T(0), T(0), T(0), T(0), T(0)};
-      const T rho_c = R(cs, 0, HR + tx, HR + ty);
       if (a.gravity_mask) {
+        const T rho_c = R(slot_of(zc), 0, HR + tx, HR + ty);
 #pragma unroll
         for (int d = 0; d < 3; ++d)
           if (a.gravity_mask & (1 << d))
@@ -332,24 +401,23 @@ __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
       T out[5];
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
+        const T fhi = fz[(v * TX + tx) * TY + ty];
         T rhs = src[v];
         rhs = rhs - (fx[(v * (TX + 1) + tx + 1) * TY + ty] -
                      fx[(v * (TX + 1) + tx) * TY + ty]) / dx;
         rhs = rhs - (fy[(v * TX + tx) * (TY + 1) + ty + 1] -
                      fy[(v * TX + tx) * (TY + 1) + ty]) / dy;
-        rhs = rhs - (fhi[v] - flo[v]) / dz;
-        const T* ukv = static_cast<const T*>(a.uk[v]);
+        rhs = rhs - (fhi - flo[v]) / dz;
+        flo[v] = fhi;
         T r;
         if (a.mode == SWC_OUT_RHS) {
           r = rhs;
         } else if (a.mode == SWC_OUT_EULER) {
-          r = __ldg(ukv + o) + rhs * dt;
+          r = ukc[v] + rhs * dt;
         } else if (a.mode == SWC_OUT_CONVEX) {
-          const T* u0v = static_cast<const T*>(a.u0[v]);
-          r = __ldg(u0v + o) * c0 + (__ldg(ukv + o) + rhs * dt) * c1;
+          r = u0c[v] * c0 + (ukc[v] + rhs * dt) * c1;
         } else {
-          const T* u0v = static_cast<const T*>(a.u0[v]);
-          r = c0 * (__ldg(u0v + o) + (__ldg(ukv + o) + dt * rhs));
+          r = c0 * (u0c[v] + (ukc[v] + dt * rhs));
         }
         out[v] = r;
       }
@@ -357,17 +425,16 @@ __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
       for (int v = 0; v < 5; ++v) static_cast<T*>(a.uout[v])[o] = out[v];
       if (a.dtmin_out) {
         T u, v, w, e, p, hh;
-        cons_to_prim(out[0], out[1], out[2], out[3], out[4], pe_at(xa, ya, za),
-                     u, v, w, e, p, hh);
+        cons_to_prim(out[0], out[1], out[2], out[3], out[4],
+                     pe_at(xa_c, ya_c, za), u, v, w, e, p, hh);
         T c = sqrt_(K<T>::gamma() * p / out[0]);
         T l = min_(min_(dx / (abs_(u) + c), dy / (abs_(v) + c)),
                    dz / (abs_(w) + c));
         dtmin_local = fmin(dtmin_local, double(l));
       }
-#pragma unroll
-      for (int v = 0; v < 5; ++v) flo[v] = fhi[v];
     }
   }
+  cp_async_wait_all();
 
   if (a.dtmin_out) {
     // Block min of the CFL limits, then one atomic per CTA.

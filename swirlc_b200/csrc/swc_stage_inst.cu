@@ -50,7 +50,7 @@ int launch_rm(const StageArgs& a, int tile, cudaStream_t st) {
   }
 #else
   (void)tile;
-  return launch_tile<T, RM, V, 32, 8>(a, st);
+  return launch_tile<T, RM, V, 16, 16>(a, st);
 #endif
 }
 
@@ -64,7 +64,7 @@ size_t smem_tile(int tile) {
   }
 #else
   (void)tile;
-  return Layout<T, SWC_SCHEME, V, 32, 8>::SMEM;
+  return Layout<T, SWC_SCHEME, V, 16, 16>::SMEM;
 #endif
 }
 
