@@ -129,7 +129,18 @@ __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
   T* fz = fx + L::FX_ELEMS;       // [5][TX][TY]
 
   const int tid = threadIdx.x;
-  const int ty = tid % TY, tx = tid / TY;
+  // Cell of this thread. For TY = 16 a warp covers rows w and w + TX/2, whose
+  // shared-memory rows are (TX/2)*PW floats apart: with PW = 22 and TX = 16
+  // that is 176 = 16 (mod 32), so the two half-warps hit disjoint banks.
+  int ty, tx;
+  if constexpr (TY == 16 && TX % 2 == 0) {
+    const int w = tid >> 5, lane = tid & 31;
+    ty = lane & 15;
+    tx = w + (lane >> 4) * (TX / 2);
+  } else {
+    ty = tid % TY;
+    tx = tid / TY;
+  }
   const int y0 = blockIdx.x * TY, x0 = blockIdx.y * TX;
   const int z0 = blockIdx.z * a.zseg;
   const int z1 = min(z0 + a.zseg, a.nz);
