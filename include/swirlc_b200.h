@@ -163,7 +163,7 @@ int swc_reconstruct(const SwcGrid* grid, int32_t dtype, int32_t interp,
 
 /* Pointwise intercell convective flux for `n` face points from reconstructed
  * primitive states. prim_neg/prim_pos hold 7 + nscalars arrays each:
- * rho, u, v, w, e, p, h, scalars. p_dyn_neg/pos may be NULL (helper p_dyn,
+ * rho, u, v, w, e, p, h, then the transported scalars phi (0..3). p_dyn_neg/pos may be NULL (helper p_dyn,
  * hllc.py:105-120). `pe` (n entries, may be NULL) is the potential energy
  * at the face index. flux holds 5 + nscalars outputs.
  * Replaces hll_convective_flux (hll.py:36-175) and hllc_convective_flux

@@ -338,7 +338,7 @@ def _limiter(r, kind):
   raise ValueError(f'Unknown limiter {kind}.')
 
 
-def muscl(v, dim, limiter='van_leer'):
+def muscl(v, dim, limiter='mc'):
   """Slope-limited MUSCL reconstruction at face i-1/2.
 
   For cell c: dp = v[c+1]-v[c], dm = v[c]-v[c-1], r = divide_no_nan(dm, dp),
@@ -367,7 +367,7 @@ def face_interp_fn(cfg):
   if scheme == 'WENO_5':
     return lambda v, d: weno(v, d, 3)
   if scheme == 'MUSCL':
-    lim = cfgget(cfg, 'muscl_limiter', 'van_leer')
+    lim = cfgget(cfg, 'muscl_limiter', 'mc')
     return lambda v, d: muscl(v, d, lim)
   if scheme == 'NODE':
     return node_interp

@@ -92,7 +92,7 @@ _DEFAULT_OPTIONS = {
         }
     },
     # Keys added by this implementation (see module docstring).
-    'muscl_limiter': 'van_leer',
+    'muscl_limiter': 'mc',
     'cfl': 0.0,
     't_end': 0.0,
 }

@@ -252,12 +252,13 @@ __global__ void recon_kernel(Geo3 g, int dim, int limiter, const T* v, T* neg,
 
 struct PointArgs {
   long long n;
-  const void* ql[7];
-  const void* qr[7];
+  int ns;  // transported scalars
+  const void* ql[7 + 3];
+  const void* qr[7 + 3];
   const void* pdl;
   const void* pdr;
   const void* pe;
-  void* out[5];
+  void* out[5 + 3];
   void* sl;
   void* sm;
   void* sr;
@@ -275,6 +276,9 @@ __device__ __forceinline__ void load_prim(const void* const* q, long long i,
   p.h = static_cast<const T*>(q[6])[i];
 }
 
+// Pointwise flux; transported scalars phi follow the generic branches of
+// the physical flux (m*phi, compressible_navier_stokes.py:419-427), of HLL
+// (hll.py:159-170) and of the HLLC star flux (hllc.py:182-192).
 template <typename T, int RM, int D>
 __global__ void riemann_kernel(const PointArgs a) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.n;
@@ -290,6 +294,44 @@ __global__ void riemann_kernel(const PointArgs a) {
     else hllc_flux<T, D>(l, r, pdl, pdr, pe, f);
 #pragma unroll
     for (int k = 0; k < 5; ++k) static_cast<T*>(a.out[k])[i] = f[k];
+    if (a.ns > 0) {
+      const T ml = l.r * l.u[D], mr = r.r * r.u[D];
+      if constexpr (RM == 0) {
+        T s_l, s_r;
+        hll_speeds<T, D>(l, r, pe, s_l, s_r);
+        T ds = s_r - s_l;
+        T t1 = dnn(min_(s_r, T(0)) - min_(s_l, T(0)), ds);
+        T t2 = T(1) - t1;
+        T t3 = dnn(s_r * abs_(s_l) - s_l * abs_(s_r), T(2) * ds);
+        for (int k = 0; k < a.ns; ++k) {
+          T pl = static_cast<const T*>(a.ql[7 + k])[i];
+          T pr = static_cast<const T*>(a.qr[7 + k])[i];
+          static_cast<T*>(a.out[5 + k])[i] =
+              t1 * (mr * pr) + t2 * (ml * pl) - t3 * (r.r * pr - l.r * pl);
+        }
+      } else {
+        Prim<T> lu = l, ru = r;
+        lu.p = pdl;
+        ru.p = pdr;
+        T s_l, s_r;
+        hll_speeds<T, D>(lu, ru, pe, s_l, s_r);
+        T s_m = hllc_contact<T, D>(lu, ru, s_l, s_r);
+        bool c1 = s_l >= T(0);
+        bool c2 = (s_l <= T(0)) && (s_m >= T(0));
+        bool c3 = (s_m <= T(0)) && (s_r >= T(0));
+        bool left = c1 || c2;
+        bool star = !c1 && (c2 || c3);
+        const Prim<T>& q = left ? l : r;
+        T s_k = left ? s_l : s_r;
+        T m = left ? ml : mr;
+        for (int k = 0; k < a.ns; ++k) {
+          T ph = static_cast<const T*>(left ? a.ql[7 + k] : a.qr[7 + k])[i];
+          T fk = m * ph;
+          if (star) fk = fk + q.r * (s_m - q.u[D]) * ph * dnn(s_k, s_k - s_m);
+          static_cast<T*>(a.out[5 + k])[i] = fk;
+        }
+      }
+    }
   }
 }
 
@@ -598,17 +640,20 @@ int swc_reconstruct(const SwcGrid* grid, int32_t dtype, int32_t interp,
   return check_launch("reconstruct");
 }
 
-static int point_args(int64_t n, const void* const* ql, const void* const* qr,
-                      const void* pe, PointArgs& a) {
+static int point_args(int64_t n, int ns, const void* const* ql,
+                      const void* const* qr, const void* pe, PointArgs& a) {
   memset(&a, 0, sizeof(a));
   if (n < 0) return fail(SWC_ERR_ARG, "negative size");
+  if (ns < 0 || ns > 3)
+    return fail(SWC_ERR_UNSUPPORTED, "%d transported scalars (at most 3)", ns);
   if (!ql || !qr) return fail(SWC_ERR_ARG, "NULL state list");
-  for (int k = 0; k < 7; ++k) {
+  for (int k = 0; k < 7 + ns; ++k) {
     if (!ql[k] || !qr[k]) return fail(SWC_ERR_ARG, "NULL primitive %d", k);
     a.ql[k] = ql[k];
     a.qr[k] = qr[k];
   }
   a.n = n;
+  a.ns = ns;
   a.pe = pe;
   return SWC_OK;
 }
@@ -622,16 +667,15 @@ int swc_riemann_flux(int64_t n, int32_t dtype, int32_t riemann, int32_t dim,
   if (riemann != SWC_HLL && riemann != SWC_HLLC)
     return fail(SWC_ERR_ARG, "numeric flux scheme %d is not implemented", riemann);
   if (dim < 0 || dim > 2) return fail(SWC_ERR_ARG, "bad dim %d", dim);
-  if (nscalars != 0) return fail(SWC_ERR_UNSUPPORTED, "scalars not supported here");
   PointArgs a;
-  int st = point_args(n, prim_neg, prim_pos, pe, a);
+  int st = point_args(n, nscalars, prim_neg, prim_pos, pe, a);
   if (st) return st;
   if ((p_dyn_neg == nullptr) != (p_dyn_pos == nullptr))
     return fail(SWC_ERR_ARG, "p_dyn needs both sides");
   a.pdl = p_dyn_neg;
   a.pdr = p_dyn_pos;
   if (!flux) return fail(SWC_ERR_ARG, "NULL flux list");
-  for (int k = 0; k < 5; ++k) {
+  for (int k = 0; k < 5 + nscalars; ++k) {
     if (!flux[k]) return fail(SWC_ERR_ARG, "NULL flux %d", k);
     a.out[k] = flux[k];
   }
@@ -661,7 +705,7 @@ int swc_wave_speeds(int64_t n, int32_t dtype, int32_t dim,
   if (!dtype_ok(dtype)) return fail(SWC_ERR_ARG, "bad dtype %d", dtype);
   if (dim < 0 || dim > 2) return fail(SWC_ERR_ARG, "bad dim %d", dim);
   PointArgs a;
-  int st = point_args(n, prim_neg, prim_pos, pe, a);
+  int st = point_args(n, 0, prim_neg, prim_pos, pe, a);
   if (st) return st;
   if (!s_l || !s_r) return fail(SWC_ERR_ARG, "NULL output");
   a.sl = s_l; a.sm = s_m; a.sr = s_r;

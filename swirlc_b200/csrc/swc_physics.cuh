@@ -193,6 +193,91 @@ __device__ __forceinline__ T muscl_slope(T vm1, T v0, T vp1, int limiter) {
 }
 
 // ---------------------------------------------------------------------------
+// Cell-centred reconstruction: both face values of one cell c from its
+// stencil s[0 .. CL+CR] = v[c-CL .. c+CR]. `right` is the neg value of face
+// c+1/2, `left` the pos value of face c-1/2. For WENO the smoothness
+// indicators and the reciprocals 1/(eps+beta_r)^2 are shared by both sides.
+// NODE keeps the identity mock's convention (face i-1/2 takes v[i] on both
+// sides), i.e. right(c) = v[c+1], left(c) = v[c].
+// ---------------------------------------------------------------------------
+template <int SCHEME>
+struct CellStencil;
+template <>
+struct CellStencil<0> {
+  static constexpr int CL = 2, CR = 2;
+};
+template <>
+struct CellStencil<1> {
+  static constexpr int CL = 1, CR = 1;
+};
+template <>
+struct CellStencil<2> {
+  static constexpr int CL = 1, CR = 1;
+};
+template <>
+struct CellStencil<3> {
+  static constexpr int CL = 0, CR = 1;
+};
+
+template <int SCHEME, typename T>
+__device__ __forceinline__ void reconstruct_cell(const T* s, int limiter,
+                                                 T& left, T& right) {
+  if constexpr (SCHEME == 0) {
+    const T vm2 = s[0], vm1 = s[1], v0 = s[2], vp1 = s[3], vp2 = s[4];
+    const T c1312 = T(13.0 / 12.0), q = T(0.25), eps = T(1e-6);
+    T a = v0 - T(2) * vp1 + vp2, b = T(3) * v0 - T(4) * vp1 + vp2;
+    T b0 = c1312 * a * a + q * b * b;
+    a = vm1 - T(2) * v0 + vp1;
+    b = vm1 - vp1;
+    T b1 = c1312 * a * a + q * b * b;
+    a = vm2 - T(2) * vm1 + v0;
+    b = vm2 - T(4) * vm1 + T(3) * v0;
+    T b2 = c1312 * a * a + q * b * b;
+    b0 += eps;
+    b1 += eps;
+    b2 += eps;
+    const T i0 = rcp_(b0 * b0), i1 = rcp_(b1 * b1), i2 = rcp_(b2 * b2);
+    {  // right face: d = (0.3, 0.6, 0.1)
+      const T a0 = T(0.3) * i0, a1 = T(0.6) * i1, a2 = T(0.1) * i2;
+      const T q0 = T(1.0 / 3.0) * v0 + T(5.0 / 6.0) * vp1 - T(1.0 / 6.0) * vp2;
+      const T q1 = T(-1.0 / 6.0) * vm1 + T(5.0 / 6.0) * v0 + T(1.0 / 3.0) * vp1;
+      const T q2 = T(1.0 / 3.0) * vm2 - T(7.0 / 6.0) * vm1 + T(11.0 / 6.0) * v0;
+      right = (a0 * q0 + a1 * q1 + a2 * q2) * rcp_(a0 + a1 + a2);
+    }
+    {  // left face: d = (0.1, 0.6, 0.3)
+      const T a0 = T(0.1) * i0, a1 = T(0.6) * i1, a2 = T(0.3) * i2;
+      const T q0 = T(11.0 / 6.0) * v0 - T(7.0 / 6.0) * vp1 + T(1.0 / 3.0) * vp2;
+      const T q1 = T(1.0 / 3.0) * vm1 + T(5.0 / 6.0) * v0 - T(1.0 / 6.0) * vp1;
+      const T q2 = T(-1.0 / 6.0) * vm2 + T(5.0 / 6.0) * vm1 + T(1.0 / 3.0) * v0;
+      left = (a0 * q0 + a1 * q1 + a2 * q2) * rcp_(a0 + a1 + a2);
+    }
+  } else if constexpr (SCHEME == 1) {
+    const T vm1 = s[0], v0 = s[1], vp1 = s[2];
+    const T eps = T(1e-6);
+    T b0 = (vp1 - v0) * (vp1 - v0) + eps;
+    T b1 = (v0 - vm1) * (v0 - vm1) + eps;
+    const T i0 = rcp_(b0 * b0), i1 = rcp_(b1 * b1);
+    {
+      const T a0 = T(2.0 / 3.0) * i0, a1 = T(1.0 / 3.0) * i1;
+      right = (a0 * (T(0.5) * v0 + T(0.5) * vp1) +
+               a1 * (T(-0.5) * vm1 + T(1.5) * v0)) * rcp_(a0 + a1);
+    }
+    {
+      const T a0 = T(1.0 / 3.0) * i0, a1 = T(2.0 / 3.0) * i1;
+      left = (a0 * (T(1.5) * v0 - T(0.5) * vp1) +
+              a1 * (T(0.5) * vm1 + T(0.5) * v0)) * rcp_(a0 + a1);
+    }
+  } else if constexpr (SCHEME == 2) {
+    const T sl = muscl_slope(s[0], s[1], s[2], limiter);
+    right = s[1] + T(0.5) * sl;
+    left = s[1] - T(0.5) * sl;
+  } else {
+    left = s[0];
+    right = s[1];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Packed single-precision reconstruction. The neg value of face i-1/2 (right
 // face of cell i-1) and its pos value (left face of cell i) use the same
 // formulas on stencils shifted by one cell, with mirrored coefficients, so

@@ -166,7 +166,7 @@ class Solver:
     sc.dtype = nat.dtype_code(dtype)
     sc.interp = (_INTERP[interp_override] if interp_override
                  else interp_code(cfg))
-    lim = getattr(cfg, 'muscl_limiter', 'van_leer')
+    lim = getattr(cfg, 'muscl_limiter', 'mc')
     if lim not in _LIMITER:
       raise ValueError(f'Unknown MUSCL limiter "{lim}".')
     sc.limiter = _LIMITER[lim]
