@@ -307,7 +307,8 @@ __global__ void riemann_kernel(const PointArgs a) {
           T pl = static_cast<const T*>(a.ql[7 + k])[i];
           T pr = static_cast<const T*>(a.qr[7 + k])[i];
           static_cast<T*>(a.out[5 + k])[i] =
-              t1 * (mr * pr) + t2 * (ml * pl) - t3 * (r.r * pr - l.r * pl);
+              t1 * (mr * pr) + t2 * (ml * pl) -
+              t3 * (mul_rn(r.r, pr) - mul_rn(l.r, pl));
         }
       } else {
         Prim<T> lu = l, ru = r;

@@ -48,6 +48,10 @@ __device__ __forceinline__ double min_(double a, double b) { return fmin(a, b); 
 __device__ __forceinline__ float max_(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double max_(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ float abs_(float a) { return fabsf(a); }
+// Products that must not be contracted into an FMA: the conserved states of
+// the two sides of a face, so that U_R - U_L is exactly 0 for equal states.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double abs_(double a) { return fabs(a); }
 
 // Primitive state at a face or a cell: rho, (u, v, w), e, p, h.
@@ -409,10 +413,13 @@ __device__ __forceinline__ void hll_speeds(const Prim<T>& l, const Prim<T>& r,
   T rl = sqrt_(l.r), rr = sqrt_(r.r);
   T den = rl + rr;
   T inv = den == T(0) ? T(0) : T(1) / den;
+  // Roe averages without FMA contraction: mirror-image states give exactly
+  // u~ = 0 (hll.py:243-261 evaluates them as separate products).
   T ru[3];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) ru[i] = (rl * l.u[i] + rr * r.u[i]) * inv;
-  T rh = (rl * l.h + rr * r.h) * inv;
+  for (int i = 0; i < 3; ++i)
+    ru[i] = (mul_rn(rl, l.u[i]) + mul_rn(rr, r.u[i])) * inv;
+  T rh = (mul_rn(rl, l.h) + mul_rn(rr, r.h)) * inv;
   T hs = rh - T(0.5) * (ru[0] * ru[0] + ru[1] * ru[1] + ru[2] * ru[2]) - pe;
   T rc = sqrt_(K<T>::gm1() * hs);
   s_l = min_(l.u[D] - c_l, ru[D] - rc);
@@ -435,8 +442,10 @@ __device__ __forceinline__ void hll_flux(const Prim<T>& l, const Prim<T>& r,
   T fl[5], fr[5];
   physical_flux<T, D>(l, pdl, fl);
   physical_flux<T, D>(r, pdr, fr);
-  T ul[5] = {l.r, l.r * l.u[0], l.r * l.u[1], l.r * l.u[2], l.r * l.e};
-  T ur[5] = {r.r, r.r * r.u[0], r.r * r.u[1], r.r * r.u[2], r.r * r.e};
+  T ul[5] = {l.r, mul_rn(l.r, l.u[0]), mul_rn(l.r, l.u[1]),
+             mul_rn(l.r, l.u[2]), mul_rn(l.r, l.e)};
+  T ur[5] = {r.r, mul_rn(r.r, r.u[0]), mul_rn(r.r, r.u[1]),
+             mul_rn(r.r, r.u[2]), mul_rn(r.r, r.e)};
 #pragma unroll
   for (int k = 0; k < 5; ++k)
     f[k] = t1 * fr[k] + t2 * fl[k] - t3 * (ur[k] - ul[k]);
@@ -447,8 +456,9 @@ template <typename T, int D>
 __device__ __forceinline__ T hllc_contact(const Prim<T>& l, const Prim<T>& r,
                                           T s_l, T s_r) {
   T vl = l.u[D], vr = r.u[D];
-  T num = r.p - l.p + l.r * vl * (s_l - vl) - r.r * vr * (s_r - vr);
-  T den = l.r * (s_l - vl) - r.r * (s_r - vr);
+  T num = (r.p - l.p) + mul_rn(mul_rn(l.r, vl), s_l - vl) -
+          mul_rn(mul_rn(r.r, vr), s_r - vr);
+  T den = mul_rn(l.r, s_l - vl) - mul_rn(r.r, s_r - vr);
   T s_m = dnn(num, den);
   return abs_(s_m) < T(1e-6) ? T(0) : s_m;
 }

