@@ -1,0 +1,94 @@
+"""CPU: the C-ABI library loads, exports every declared symbol, and its
+struct layouts match the ctypes mirror (no kernel is launched)."""
+
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from swirlc_b200 import _native as nat
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, 'include', 'swirlc_b200.h')
+
+
+def _declared():
+  with open(HEADER) as f:
+    text = f.read()
+  return sorted(set(re.findall(r'\b(swc_\w+)\s*\(', text)))
+
+
+@pytest.fixture(scope='module')
+def lib():
+  if not os.path.exists(nat.lib_path()):
+    from swirlc_b200 import build
+    build.build()
+  return nat.load(require_cuda=False)
+
+
+def test_every_declared_symbol_is_exported(lib):
+  names = _declared()
+  assert set(names) == set(nat.EXPORTED)
+  for name in names:
+    assert hasattr(lib, name), name
+
+
+def test_abi_version_and_error_buffer(lib):
+  assert lib.swc_abi_version() == 1
+  buf = ctypes.create_string_buffer(64)
+  assert lib.swc_last_error(buf, len(buf)) >= 0
+
+
+def test_argument_errors_need_no_gpu(lib):
+  # Validation runs before any CUDA call and maps to ValueError.
+  with pytest.raises(ValueError):
+    nat.check(lib.swc_rk_stage(None, None, None, None, None, 0, 0.0, 0.0,
+                               None, None, None))
+  with pytest.raises(ValueError):
+    nat.check(lib.swc_clock_begin_step(None, None))
+
+
+def _c_layout():
+  src = r'''
+#include <stddef.h>
+#include <stdio.h>
+#include "swirlc_b200.h"
+#define F(T, m) printf(#T "." #m " %zu\n", offsetof(T, m));
+int main(void) {
+  printf("SwcGrid %zu\n", sizeof(SwcGrid));
+  printf("SwcScheme %zu\n", sizeof(SwcScheme));
+  printf("SwcBC %zu\n", sizeof(SwcBC));
+  printf("SwcFieldBC %zu\n", sizeof(SwcFieldBC));
+  printf("SwcClock %zu\n", sizeof(SwcClock));
+  F(SwcGrid, sx) F(SwcGrid, dz) F(SwcScheme, nu) F(SwcScheme, g)
+  F(SwcScheme, pe_axis) F(SwcScheme, zseg) F(SwcBC, value) F(SwcBC, planes)
+  F(SwcFieldBC, side) F(SwcClock, step)
+  return 0;
+}
+'''
+  with tempfile.TemporaryDirectory() as d:
+    c = os.path.join(d, 'layout.c')
+    exe = os.path.join(d, 'layout')
+    with open(c, 'w') as f:
+      f.write(src)
+    subprocess.run(['gcc', '-I', os.path.join(ROOT, 'include'), c, '-o', exe],
+                   check=True)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True)
+  return dict(line.rsplit(' ', 1) for line in out.stdout.strip().splitlines())
+
+
+def test_struct_layouts_match_header():
+  c = {k: int(v) for k, v in _c_layout().items()}
+  assert c['SwcGrid'] == ctypes.sizeof(nat.SwcGrid)
+  assert c['SwcScheme'] == ctypes.sizeof(nat.SwcScheme)
+  assert c['SwcBC'] == ctypes.sizeof(nat.SwcBC)
+  assert c['SwcFieldBC'] == ctypes.sizeof(nat.SwcFieldBC)
+  assert c['SwcClock'] == ctypes.sizeof(nat.SwcClock)
+  for key, off in c.items():
+    if '.' not in key:
+      continue
+    st, field = key.split('.')
+    assert getattr(getattr(nat, st), field).offset == off, key
