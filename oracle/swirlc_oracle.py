@@ -150,13 +150,14 @@ def potential_energy(cfg, shape, dtype, core_idx=(0, 0, 0)) -> np.ndarray:
   """generic.py:282-319: e_g = -g_vec . x on the cell-centre mesh."""
   if gravity_direction(cfg) == -1:
     return np.zeros(shape, dtype=dtype)
-  mesh = mesh_local(cfg, core_idx, dtype)
+  mesh = mesh_local(cfg, core_idx, np.dtype(dtype).type)
   g = cfgget(cfg, 'g')
   g_vec = G * np.array([g[d] for d in DIMS], dtype=float)
   x = mesh['x'][np.newaxis, :, np.newaxis]
   y = mesh['y'][np.newaxis, np.newaxis, :]
   z = mesh['z'][:, np.newaxis, np.newaxis]
-  pe = (-dtype(g_vec[0]) * x - dtype(g_vec[1]) * y) - dtype(g_vec[2]) * z
+  t = np.dtype(dtype).type
+  pe = (-t(g_vec[0]) * x - t(g_vec[1]) * y) - t(g_vec[2]) * z
   return np.broadcast_to(pe, shape).astype(dtype)
 
 
