@@ -57,7 +57,7 @@ def _peaks():
 
 def _traffic_from_profiles():
   """Per-launch DRAM bytes of the stage kernel from the committed ncu summary."""
-  path = os.path.join(ROOT, 'profiles', 'stage_kernel_kh.txt')
+  path = os.path.join(ROOT, 'profiles', 'stage_kernel_kh256.txt')
   try:
     with open(path) as f:
       for line in f:
@@ -88,7 +88,7 @@ class ClockSampler:
     try:
       self.proc = subprocess.Popen(
           ['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.Q}',
-           '--format=csv,noheader,nounits', '-lms', '200'],
+           '--format=csv,noheader,nounits', '-lms', '50'],
           stdout=open(self.path, 'w'), stderr=subprocess.DEVNULL)
     except OSError:
       self.proc = None
@@ -272,6 +272,23 @@ def run_ours(args):
     dist.destroy_process_group()
 
 
+def run_profile(args):
+  """Eager RK3 steps of the workload, no timing: the command ncu captures."""
+  import torch
+  from swirlc_b200 import configs, engine
+  from swirlc_b200.core import parameter
+  from swirlc_b200.physics import physics_models
+  user_cfg, state = configs.kelvin_helmholtz(n=args.n)
+  cfg = parameter.SwirlCParameters(user_cfg)
+  pm = physics_models.PhysicsModels(cfg)
+  fields = [torch.tensor(state[k], device='cuda') for k in
+            ('rho', 'rho_u', 'rho_v', 'rho_w', 'rho_e')]
+  solver = engine.Solver(cfg, pm, fields[0].shape, torch.float32)
+  stepper = engine.Stepper(solver, fields, dt=cfg.dt, cfl=cfg.cfl)
+  stepper.step(args.profile_steps)
+  torch.cuda.synchronize()
+
+
 def _oracle_rk3_worker(payload):
   import numpy as _np
   from oracle import swirlc_oracle as orc
@@ -348,7 +365,13 @@ def main():
   ap.add_argument('--n', type=int, default=N_CELLS_EDGE)
   ap.add_argument('--cpu-sample', type=int, default=96)
   ap.add_argument('--no-cpu-baseline', action='store_true')
+  ap.add_argument('--profile-steps', type=int, default=0,
+                  help='only run this many eager RK3 steps of the workload '
+                       '(a small, untimed command for ncu captures)')
   args = ap.parse_args()
+  if args.profile_steps:
+    run_profile(args)
+    return
   if args.warmup < 3:
     args.warmup = 3
   if args.impl == 'reference':
