@@ -139,6 +139,20 @@ int swc_rk_stage(const SwcGrid* grid, const SwcScheme* scheme,
                  void* const* uout, int32_t mode, double c0, double c1,
                  const double* dt, double* dtmin_out, void* stream);
 
+/* One time step in place on `u` (5 fields): [clock begin] -> halo fill ->
+ * fused stages -> [clock end]. order 3: SSP-RK3 (rk3.py:87-120); order 2:
+ * RK2 (rk2.py:69-86). `work` holds 10 field buffers (two states of the
+ * shape of u) used as scratch. `clock_dev` is a device SwcClock: the step
+ * uses clock->dt; with clock->cfl > 0 the step starts with
+ * dt = min(cfl*dtmin, t_end-t) and its last stage min-reduces the CFL limit
+ * of the new state into clock->dtmin for the next step (so before the first
+ * step clock->dtmin must hold the limit of the initial state, e.g. from
+ * swc_cfl_reduce). Replaces Simulation.step (simulation.py:68-105) for one
+ * replica. */
+int swc_rk_step(const SwcGrid* grid, const SwcScheme* scheme,
+                const SwcFieldBC* bcs, int32_t order, void* const* u,
+                void* const* work, SwcClock* clock_dev, void* stream);
+
 /* dtmin_out <- min(dtmin_out, min over interior cells and dims of
  * delta_d / (|u_d| + c)), c = sqrt(gamma p / rho) (CFL rule of the
  * reference's prototype, demo/swirl_c_prototype.ipynb `solve`). */

@@ -39,7 +39,7 @@ EXPORTED = (
     'swc_abi_version', 'swc_last_error', 'swc_launch_count', 'swc_halo_fill',
     'swc_rk_stage', 'swc_cfl_reduce', 'swc_clock_begin_step',
     'swc_clock_end_step', 'swc_reconstruct', 'swc_riemann_flux',
-    'swc_wave_speeds', 'swc_stencil', 'swc_rk_combine',
+    'swc_wave_speeds', 'swc_stencil', 'swc_rk_combine', 'swc_rk_step',
 )
 
 
@@ -122,6 +122,10 @@ def load(require_cuda: bool = True) -> ctypes.CDLL:
                                   vp, vp, vp]
       lib.swc_rk_combine.argtypes = [i64, i32, i32, dbl, dbl, vp, vp, vp, vp,
                                      vp, vp]
+      lib.swc_rk_step.argtypes = [ctypes.POINTER(SwcGrid),
+                                  ctypes.POINTER(SwcScheme),
+                                  ctypes.POINTER(SwcFieldBC), i32, pp, pp, vp,
+                                  vp]
       for name in EXPORTED:
         fn = getattr(lib, name)
         if fn.restype is ctypes.c_int and name not in ('swc_abi_version',):

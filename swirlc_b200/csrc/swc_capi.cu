@@ -772,4 +772,53 @@ int swc_rk_combine(int64_t n, int32_t dtype, int32_t mode, double c0,
   return check_launch("rk_combine");
 }
 
+int swc_rk_step(const SwcGrid* grid, const SwcScheme* scheme,
+                const SwcFieldBC* bcs, int32_t order, void* const* u,
+                void* const* work, SwcClock* clock_dev, void* stream) {
+  int st = check_grid(grid);
+  if (st) return st;
+  if (!scheme || !bcs || !u || !work || !clock_dev)
+    return fail(SWC_ERR_ARG, "NULL argument");
+  if (order != 2 && order != 3)
+    return fail(SWC_ERR_UNSUPPORTED, "Runge-Kutta order %d is not implemented",
+                order);
+  for (int v = 0; v < 5; ++v) {
+    if (!u[v]) return fail(SWC_ERR_ARG, "NULL field %d", v);
+    if (!work[v] || !work[5 + v]) return fail(SWC_ERR_ARG, "NULL work buffer");
+  }
+  void* w1[5];
+  void* w2[5];
+  for (int v = 0; v < 5; ++v) {
+    w1[v] = work[v];
+    w2[v] = work[5 + v];
+  }
+  const double* dt = &clock_dev->dt;
+  double* dtmin = &clock_dev->dtmin;
+  if ((st = swc_clock_begin_step(clock_dev, stream))) return st;
+  if ((st = swc_halo_fill(grid, scheme->dtype, 5, u, bcs, 0, stream))) return st;
+  if ((st = swc_rk_stage(grid, scheme, (const void* const*)u, nullptr, w1,
+                         SWC_OUT_EULER, 0.0, 0.0, dt, nullptr, stream)))
+    return st;
+  if ((st = swc_halo_fill(grid, scheme->dtype, 5, w1, bcs, 0, stream)))
+    return st;
+  if (order == 3) {
+    if ((st = swc_rk_stage(grid, scheme, (const void* const*)w1,
+                           (const void* const*)u, w2, SWC_OUT_CONVEX, 0.75,
+                           0.25, dt, nullptr, stream)))
+      return st;
+    if ((st = swc_halo_fill(grid, scheme->dtype, 5, w2, bcs, 0, stream)))
+      return st;
+    if ((st = swc_rk_stage(grid, scheme, (const void* const*)w2,
+                           (const void* const*)u, u, SWC_OUT_CONVEX,
+                           1.0 / 3.0, 2.0 / 3.0, dt, dtmin, stream)))
+      return st;
+  } else {
+    if ((st = swc_rk_stage(grid, scheme, (const void* const*)w1,
+                           (const void* const*)u, u, SWC_OUT_AVERAGE, 0.5, 0.0,
+                           dt, dtmin, stream)))
+      return st;
+  }
+  return swc_clock_end_step(clock_dev, stream);
+}
+
 }  // extern "C"

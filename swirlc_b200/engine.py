@@ -341,25 +341,13 @@ class Stepper:
     return self.clock[1:2]
 
   def _launch_step(self):
-    s, lib = self.s, nat.load()
-    st = nat.stream_ptr()
-    cptr = self.clock.data_ptr()
-    if self.cfl > 0.0:
-      nat.check(lib.swc_clock_begin_step(cptr, st), 'clock')
-    dt = self.clock[1:2]
-    dtmin = self.clock[2:3] if self.cfl > 0.0 else None
-    s.fill_halos(self.u)
-    s.stage(self.u, None, self.w1, nat.SWC_OUT_EULER, dt=dt)
-    s.fill_halos(self.w1)
-    if self.scheme == 'rk3':
-      s.stage(self.w1, self.u, self.w2, nat.SWC_OUT_CONVEX, 0.75, 0.25, dt=dt)
-      s.fill_halos(self.w2)
-      s.stage(self.w2, self.u, self.u, nat.SWC_OUT_CONVEX, 1.0 / 3.0,
-              2.0 / 3.0, dt=dt, dtmin_out=dtmin)
-    else:
-      s.stage(self.w1, self.u, self.u, nat.SWC_OUT_AVERAGE, 0.5, 0.0, dt=dt,
-              dtmin_out=dtmin)
-    nat.check(lib.swc_clock_end_step(cptr, st), 'clock')
+    """One step through swc_rk_step (halo fills, fused stages, clock)."""
+    work = self.w1 + self.w2
+    nat.check(nat.load().swc_rk_step(
+        ctypes.byref(self.s.grid), ctypes.byref(self.s.scheme), self.s.bcs,
+        3 if self.scheme == 'rk3' else 2, nat.ptr_array(self.u),
+        nat.ptr_array(work), self.clock.data_ptr(), nat.stream_ptr()),
+        'rk step')
 
   def capture(self) -> None:
     """Captures one step in a CUDA graph (after one eager warm-up step)."""
