@@ -153,6 +153,30 @@ int swc_rk_step(const SwcGrid* grid, const SwcScheme* scheme,
                 const SwcFieldBC* bcs, int32_t order, void* const* u,
                 void* const* work, SwcClock* clock_dev, void* stream);
 
+/* Size of the built-in work space of swc_rk_step_noalloc (64 MiB). */
+#define SWC_NOALLOC_MAX_BYTES (64ll << 20)
+
+/* swc_rk_step without the `work` argument; it has no counterpart in the
+ * reference. It is for callers that cannot provide the ten work buffers:
+ * hosts that must not allocate device memory while running (a plugin whose
+ * host owns and budgets all device memory, a real-time loop where an
+ * allocation could block or fail) and bindings with no CUDA allocator. The
+ * work states live in one array of SWC_NOALLOC_MAX_BYTES inside this library,
+ * held on every GPU that loads it until the process exits; the call itself
+ * allocates nothing. Grids whose ten padded fields (10 * sz * (nz + 2*halo)
+ * elements, each field rounded up to 256 bytes) exceed it are rejected with
+ * SWC_ERR_ARG before anything is launched (e.g. 96^3 f32 with halo 3 fits,
+ * 128^3 does not). The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress with that device current); make that call
+ * before any stream capture. All calls share the array, which keeps the last
+ * call's contents, so calls that overlap on the GPU race: serialise them
+ * (one stream, or events between streams and threads). Nothing in the array
+ * needs to be zero; halo sides set to SWC_BC_NONE keep whatever the array
+ * held there. */
+int swc_rk_step_noalloc(const SwcGrid* grid, const SwcScheme* scheme,
+                        const SwcFieldBC* bcs, int32_t order, void* const* u,
+                        SwcClock* clock_dev, void* stream);
+
 /* dtmin_out <- min(dtmin_out, min over interior cells and dims of
  * delta_d / (|u_d| + c)), c = sqrt(gamma p / rho) (CFL rule of the
  * reference's prototype, demo/swirl_c_prototype.ipynb `solve`). */

@@ -40,7 +40,11 @@ EXPORTED = (
     'swc_rk_stage', 'swc_cfl_reduce', 'swc_clock_begin_step',
     'swc_clock_end_step', 'swc_reconstruct', 'swc_riemann_flux',
     'swc_wave_speeds', 'swc_stencil', 'swc_rk_combine', 'swc_rk_step',
+    'swc_rk_step_noalloc',
 )
+
+# Built-in work space of swc_rk_step_noalloc (SWC_NOALLOC_MAX_BYTES).
+SWC_NOALLOC_MAX_BYTES = 64 << 20
 
 
 class SwcGrid(ctypes.Structure):
@@ -126,6 +130,10 @@ def load(require_cuda: bool = True) -> ctypes.CDLL:
                                   ctypes.POINTER(SwcScheme),
                                   ctypes.POINTER(SwcFieldBC), i32, pp, pp, vp,
                                   vp]
+      lib.swc_rk_step_noalloc.argtypes = [ctypes.POINTER(SwcGrid),
+                                          ctypes.POINTER(SwcScheme),
+                                          ctypes.POINTER(SwcFieldBC), i32, pp,
+                                          vp, vp]
       for name in EXPORTED:
         fn = getattr(lib, name)
         if fn.restype is ctypes.c_int and name not in ('swc_abi_version',):

@@ -37,4 +37,7 @@ inline int stage_halo_needed(int scheme, int visc) {
 // Counts kernel launches issued by this library (thread-local).
 void note_launch(int n = 1);
 
+// Sets the message swc_last_error() reports on this thread; returns `code`.
+int record_error(int code, const char* fmt, ...);
+
 }  // namespace swc

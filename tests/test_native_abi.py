@@ -49,6 +49,15 @@ def test_argument_errors_need_no_gpu(lib):
                                None, None, None))
   with pytest.raises(ValueError):
     nat.check(lib.swc_clock_begin_step(None, None))
+  with pytest.raises(ValueError):
+    nat.check(lib.swc_rk_step_noalloc(None, None, None, 3, None, None, None))
+
+
+def test_noalloc_limit_matches_header():
+  with open(os.path.join(ROOT, 'include', 'swirlc_b200.h')) as f:
+    text = f.read()
+  m = re.search(r'#define SWC_NOALLOC_MAX_BYTES \((\d+)ll << (\d+)\)', text)
+  assert m and int(m.group(1)) << int(m.group(2)) == nat.SWC_NOALLOC_MAX_BYTES
 
 
 def _c_layout():
