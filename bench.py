@@ -6,6 +6,7 @@ unit cube of 256^3 interior cells, float32, WENO5-JS + HLLC + viscous
 Seeded synthetic initial condition (swirlc_b200.configs.kelvin_helmholtz).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload kh256|riemann_batch]
 
 Under torchrun each rank advances its own 256^3 domain (weak scaling,
 replicas; the halo exchange of a decomposed domain is a separate path).
@@ -272,6 +273,206 @@ def run_ours(args):
     dist.destroy_process_group()
 
 
+BATCH_METRIC = ('RK3 cell-updates/s, 64 batched quasi-1-D Riemann problems '
+                'fp32 WENO5+HLLC, per-member CFL dt')
+
+
+def _plain_rate(configs, engine, parameter, physics_models, user_cfg, state,
+                steps):
+  """cell-updates/s of the single-grid step (one-step CUDA graph)."""
+  import torch
+  cfg = parameter.SwirlCParameters(user_cfg)
+  s = engine.Solver(cfg, physics_models.PhysicsModels(cfg), state['rho'].shape)
+  f = [torch.tensor(state[k], device='cuda') for k in
+       ('rho', 'rho_u', 'rho_v', 'rho_w', 'rho_e')]
+  st = engine.Stepper(s, f, dt=cfg.dt, cfl=cfg.cfl)
+  st.step(1)
+  st.capture()
+  st.step(3)
+  a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+  torch.cuda.synchronize()
+  a.record()
+  st.step(steps)
+  b.record()
+  torch.cuda.synchronize()
+  return s.nx * s.ny * s.nz * steps / (a.elapsed_time(b) / 1e3)
+
+
+def _batch_cpu_sample(members, procs: int = 1):
+  """CPU oracle: one SSP-RK3 step of each of the members (float32)."""
+  import multiprocessing as mp
+  from oracle import swirlc_oracle as orc
+  keys = ('halo_width', 'dx', 'dy', 'dz', 'interpolation_scheme',
+          'numeric_flux_scheme', 'include_diffusion', 'transport_parameters',
+          'x', 'y', 'z', 'bc', 'dt')
+  work, cells = [], 0
+  for cfg, state in members:
+    ocfg = orc.make_cfg(**{k: cfg[k] for k in keys if k in cfg})
+    work.append((ocfg, {k: np.asarray(v, np.float32) for k, v in state.items()}))
+    cells += cfg['nx'] * cfg['ny'] * cfg['nz']
+  t0 = time.perf_counter()
+  if procs <= 1:
+    for w in work:
+      _oracle_rk3_worker(w)
+  else:
+    with mp.get_context('spawn').Pool(procs) as pool:
+      pool.map(_oracle_rk3_worker, work)
+  secs = time.perf_counter() - t0
+  return cells / secs, secs, cells
+
+
+def _batch_sample_members(configs):
+  return [m for m in configs.riemann_batch() if m[0]['nx'] * m[0]['ny'] *
+          m[0]['nz'] <= 120000]
+
+
+def run_batch(args):
+  """The 64-member Riemann batch (configs.riemann_batch) stepped by
+  swc_batch_step under a CUDA graph; each rank runs its own batch (seed =
+  rank)."""
+  import torch
+  import torch.distributed as dist
+  from swirlc_b200 import _native as nat
+  from swirlc_b200 import batch, configs, engine
+  from swirlc_b200.core import parameter
+  from swirlc_b200.physics import physics_models
+
+  rank, world, local = _env_rank()
+  torch.cuda.set_device(local)
+  if world > 1:
+    dist.init_process_group('nccl', timeout=__import__('datetime').timedelta(seconds=120))
+  members = configs.riemann_batch(seed=rank)
+  bs = batch.BatchStepper(members)
+  cells = bs.cells()
+  bs.step(1)
+  tune = bs.autotune(steps=2, reps=2)
+  torch.cuda.synchronize()
+  c0 = nat.launch_count()
+  bs.capture(steps=1)
+  launches_per_step = nat.launch_count() - c0
+  bs.step(max(args.warmup - 1, 1))
+  torch.cuda.synchronize()
+
+  def barrier():
+    if world > 1:
+      dist.barrier()
+
+  sampler = ClockSampler(local)
+  sampler.start()
+  barrier()
+  torch.cuda.synchronize()
+  ev0, ev1 = (torch.cuda.Event(enable_timing=True) for _ in range(2))
+  ev0.record()
+  bs.step(args.steps)
+  ev1.record()
+  torch.cuda.synchronize()
+  barrier()
+  clocks = sampler.stop()
+  ms = ev0.elapsed_time(ev1)
+  if world > 1:
+    t = torch.tensor([ms], device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+  value = world * cells * args.steps / (ms / 1e3)
+  bs.graph = None
+
+  # Reference points on this GPU: the members one after another, and the
+  # plain single-grid kernel on large grids of the same scheme.
+  seq = batch.sequential_plain(members, args.steps)
+  sod_cfg, sod_state = configs.sod(n=4096, ny=32, nz=32)
+  plain_thin = _plain_rate(configs, engine, parameter, physics_models,
+                           dict(sod_cfg, t_end=0.0), sod_state, args.steps)
+  kh_cfg, kh_state = configs.kelvin_helmholtz(n=256)
+  plain_cube = _plain_rate(configs, engine, parameter, physics_models,
+                           dict(kh_cfg, include_diffusion=False), kh_state,
+                           max(5, args.steps // 2))
+
+  # End to end: every member's state from pinned host memory, one batch
+  # step, every member's state back to pinned host memory.
+  names = ('rho', 'rho_u', 'rho_v', 'rho_w', 'rho_e')
+  host = [[torch.from_numpy(np.ascontiguousarray(st[k], np.float32)).pin_memory()
+           for k in names] for _, st in members]
+  back = [[torch.empty_like(h).pin_memory() for h in hs] for hs in host]
+  e2e_steps = max(1, min(args.steps, 5))
+
+  def e2e_once():
+    for u, hs in zip(bs.u, host):
+      for f, h in zip(u, hs):
+        f.copy_(h, non_blocking=True)
+    bs.step(1)
+    for u, hs in zip(bs.u, back):
+      for f, h in zip(u, hs):
+        h.copy_(f, non_blocking=True)
+
+  e2e_once()
+  torch.cuda.synchronize()
+  barrier()
+  ea, eb = (torch.cuda.Event(enable_timing=True) for _ in range(2))
+  ea.record()
+  for _ in range(e2e_steps):
+    e2e_once()
+  eb.record()
+  torch.cuda.synchronize()
+  e2e_ms = ea.elapsed_time(eb)
+  if world > 1:
+    t = torch.tensor([e2e_ms], device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+  state_bytes = sum(h.numel() * 4 for hs in host for h in hs)
+
+  cpu = None
+  if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    sample = _batch_sample_members(configs)
+    rate, secs, scells = _batch_cpu_sample(sample)
+    cpu = {'value': rate, 'unit': UNIT, 'cores': 1, 'kind': 'port',
+           'sample': f'one SSP-RK3 step of the {len(sample)} members with '
+                     f'<= 120k cells ({scells} cells), NumPy float32 oracle, '
+                     f'{secs:.1f} s'}
+  peak, peak_kind = _peaks()
+  achieved = ALG_BYTES_PER_CELL_UPDATE * cells * args.steps / (ms / 1e3) / 1e9
+  if rank == 0:
+    line = {
+        'metric': BATCH_METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world,
+        'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': ms / args.steps, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+        'data': 'synthetic (seeded members, configs.riemann_batch)',
+        'config': {'workload': 'riemann_batch: 64 members, nx log-uniform '
+                               '[64, 4096], ny = nz in {4, 8, 16, 32}, '
+                               'WENO5+HLLC, SSP-RK3, CFL 0.5 per member',
+                   'cells_per_gpu': cells, 'members': bs.n_members,
+                   'parallelism': f'replicas x{world}',
+                   'l2_flush': 'inputs larger than L2 (3 states x 5 fields '
+                               'of all members = 1.9 GB)',
+                   'graph': 'one batch step captured in a CUDA graph',
+                   'autotune': {'small_ny': tune['small_ny'],
+                                'zseg': tune['zseg']}},
+        'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak,
+                     'unit': 'GB/s', 'frac': achieved / peak,
+                     'peak_source': peak_kind, 'traffic': None,
+                     'kernel': 'whole batch step (stage_batch_kernel + '
+                               'halo_batch_kernel), algorithmic 160 B per '
+                               'cell-update'},
+        'plain_kernel': {'sod_4096x32x32': plain_thin,
+                         'kh_256^3_inviscid': plain_cube,
+                         'batch_over_kh256': value / world / plain_cube,
+                         'batch_over_same_shape': value / world / plain_thin},
+        'sequential_members': {'value': seq['cell_updates_per_s'], 'unit': UNIT,
+                               'how': 'each member its own one-step graph, '
+                                      'members one after another'},
+        'cpu_baseline': cpu,
+        'e2e': {'value': world * cells * e2e_steps / (e2e_ms / 1e3), 'unit': UNIT,
+                'h2d_bytes_per_step': state_bytes,
+                'd2h_bytes_per_step': state_bytes,
+                'api': 'swirlc_b200.batch.BatchStepper.step'},
+        'gpu_launches': launches_per_step * args.steps,
+        'clocks': clocks,
+    }
+    print(json.dumps(line), flush=True)
+  if world > 1:
+    dist.destroy_process_group()
+
+
 def run_profile(args):
   """Eager RK3 steps of the workload, no timing: the command ncu captures."""
   import torch
@@ -326,9 +527,39 @@ def cpu_baseline_sample(n_sample: int, procs: int = 1):
                     f'{secs:.1f} s wall'}
 
 
+def run_reference_batch(args):
+  from swirlc_b200 import configs
+  procs = os.cpu_count() or 1
+  sample = _batch_sample_members(configs)
+  rates = []
+  for _ in range(max(1, min(args.steps, 3))):
+    rate, secs, scells = _batch_cpu_sample(sample, procs)
+    rates.append(rate)
+  v = statistics.median(rates)
+  desc = (f'one SSP-RK3 step of the {len(sample)} members with <= 120k cells '
+          f'({scells} cells) over {procs} processes, NumPy float32 oracle')
+  line = {
+      'impl': 'reference', 'metric': BATCH_METRIC, 'value': v, 'unit': UNIT,
+      'n_gpus': int(os.environ.get('WORLD_SIZE', '1')), 'steps': args.steps,
+      'warmup': args.warmup, 'ms_per_step': scells / v * 1e3,
+      'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+      'dtype': 'f32', 'data': 'synthetic (seeded members)',
+      'config': {'workload': 'riemann_batch (CPU sample)',
+                 'parallelism': f'{procs} host processes'},
+      'cpu_baseline': {'value': v, 'unit': UNIT, 'cores': procs,
+                       'kind': 'port', 'sample': desc},
+      'e2e': {'value': v, 'unit': UNIT, 'h2d_bytes_per_step': 0,
+              'd2h_bytes_per_step': 0},
+  }
+  print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
   rank, world, _ = _env_rank()
   if rank != 0:
+    return
+  if args.workload == 'riemann_batch':
+    run_reference_batch(args)
     return
   procs = os.cpu_count() or 1
   vals = []
@@ -365,6 +596,10 @@ def main():
   ap.add_argument('--n', type=int, default=N_CELLS_EDGE)
   ap.add_argument('--cpu-sample', type=int, default=96)
   ap.add_argument('--no-cpu-baseline', action='store_true')
+  ap.add_argument('--workload', default='kh256',
+                  choices=['kh256', 'riemann_batch'],
+                  help='kh256: the headline 256^3 Kelvin-Helmholtz step; '
+                       'riemann_batch: 64 batched Riemann problems')
   ap.add_argument('--profile-steps', type=int, default=0,
                   help='only run this many eager RK3 steps of the workload '
                        '(a small, untimed command for ncu captures)')
@@ -376,6 +611,8 @@ def main():
     args.warmup = 3
   if args.impl == 'reference':
     run_reference(args)
+  elif args.workload == 'riemann_batch':
+    run_batch(args)
   else:
     run_ours(args)
 

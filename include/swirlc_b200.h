@@ -72,7 +72,7 @@ typedef struct SwcScheme {
   int32_t nscalars;  /* transported scalars after rho_e (0..3)              */
   int32_t gravity_mask; /* bit d set: rho_u_d gets rho*G*g[d] (gravity.py:51-102) */
   int32_t zseg;      /* z planes per CTA in the stage kernel; 0 = automatic */
-  int32_t tile;      /* stage tile shape: 0 = 32x8 (y x x), 1 = 16x16, 2 = 8x32 */
+  int32_t tile;      /* unused by the single-grid stage (16x16 y x x cells)  */
   int32_t reserved;
   double nu, pr;     /* transport_parameters (simple.py:44-45)              */
   double g[3];       /* cfg.g, the gravity unit vector                      */
@@ -176,6 +176,33 @@ int swc_rk_step(const SwcGrid* grid, const SwcScheme* scheme,
 int swc_rk_step_noalloc(const SwcGrid* grid, const SwcScheme* scheme,
                         const SwcFieldBC* bcs, int32_t order, void* const* u,
                         SwcClock* clock_dev, void* stream);
+
+/* One member of a batch: an independent grid with its own state, work
+ * buffers, halo BCs, potential energy and clock. */
+typedef struct SwcBatchMember {
+  SwcGrid grid;
+  void* u[5];             /* conserved state (device), updated in place     */
+  void* work[10];         /* two work states of the shape of u (device)     */
+  const void* pe_axis[3]; /* as SwcScheme.pe_axis, for this member's mesh   */
+  SwcFieldBC bcs[5];      /* halo BCs of rho..rho_e (read during the call)  */
+  SwcClock* clock;        /* this member's device clock (own CFL dt)        */
+  int32_t tile;           /* cells per CTA (y x x): 0 or 1 16x16, 2 8x32    */
+  int32_t zseg;           /* z planes per CTA; 0 auto                       */
+} SwcBatchMember;
+
+/* One time step of every member (order 3: SSP-RK3, order 2: RK2), each with
+ * the dt of its own clock, as swc_rk_step does for one grid. All members
+ * share `scheme` (its pe_axis, tile and zseg are replaced by the members').
+ * Each RK stage is one batched halo pass per dim and one batched stage
+ * launch per tile shape over all members, instead of a launch sequence per
+ * member. With 16x16 tiles each member's result equals swc_rk_step's bit for
+ * bit; 8x32 tiles (for members at most 8 cells wide in y; not available for
+ * f64 WENO5) can differ from it in the last bit. Members must not share
+ * buffers. No counterpart in the reference, which advances
+ * one grid per program: replaces calling Simulation.step
+ * (simulation.py:68-105) on each member in turn. */
+int swc_batch_step(const SwcScheme* scheme, int32_t order, int32_t nmembers,
+                   const SwcBatchMember* members, void* stream);
 
 /* dtmin_out <- min(dtmin_out, min over interior cells and dims of
  * delta_d / (|u_d| + c)), c = sqrt(gamma p / rho) (CFL rule of the

@@ -40,7 +40,7 @@ EXPORTED = (
     'swc_rk_stage', 'swc_cfl_reduce', 'swc_clock_begin_step',
     'swc_clock_end_step', 'swc_reconstruct', 'swc_riemann_flux',
     'swc_wave_speeds', 'swc_stencil', 'swc_rk_combine', 'swc_rk_step',
-    'swc_rk_step_noalloc',
+    'swc_rk_step_noalloc', 'swc_batch_step',
 )
 
 # Built-in work space of swc_rk_step_noalloc (SWC_NOALLOC_MAX_BYTES).
@@ -79,6 +79,13 @@ class SwcClock(ctypes.Structure):
   _fields_ = [('t', ctypes.c_double), ('dt', ctypes.c_double),
               ('dtmin', ctypes.c_double), ('cfl', ctypes.c_double),
               ('t_end', ctypes.c_double), ('step', ctypes.c_int64)]
+
+
+class SwcBatchMember(ctypes.Structure):
+  _fields_ = [('grid', SwcGrid), ('u', ctypes.c_void_p * 5),
+              ('work', ctypes.c_void_p * 10), ('pe_axis', ctypes.c_void_p * 3),
+              ('bcs', SwcFieldBC * 5), ('clock', ctypes.c_void_p),
+              ('tile', ctypes.c_int32), ('zseg', ctypes.c_int32)]
 
 
 _lib: Optional[ctypes.CDLL] = None
@@ -130,6 +137,8 @@ def load(require_cuda: bool = True) -> ctypes.CDLL:
                                   ctypes.POINTER(SwcScheme),
                                   ctypes.POINTER(SwcFieldBC), i32, pp, pp, vp,
                                   vp]
+      lib.swc_batch_step.argtypes = [ctypes.POINTER(SwcScheme), i32, i32,
+                                     ctypes.POINTER(SwcBatchMember), vp]
       lib.swc_rk_step_noalloc.argtypes = [ctypes.POINTER(SwcGrid),
                                           ctypes.POINTER(SwcScheme),
                                           ctypes.POINTER(SwcFieldBC), i32, pp,

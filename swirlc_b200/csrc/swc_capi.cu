@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <string>
 
+#include "swc_halo.cuh"
 #include "swc_launch.h"
 #include "swirlc_b200.h"
 
@@ -48,7 +49,7 @@ static int check_launch(const char* what) {
   return SWC_OK;
 }
 
-static int check_grid(const SwcGrid* g) {
+int check_grid(const SwcGrid* g) {
   if (!g) return fail(SWC_ERR_ARG, "grid is NULL");
   if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || g->halo < 0)
     return fail(SWC_ERR_ARG, "bad grid sizes nx=%d ny=%d nz=%d halo=%d", g->nx,
@@ -65,82 +66,15 @@ static bool dtype_ok(int d) { return d == SWC_F32 || d == SWC_F64; }
 // ---------------------------------------------------------------------------
 // Halo fill (boundary.py:34-86, 464-539).
 // ---------------------------------------------------------------------------
-struct HaloField {
-  void* f;
-  int via_prim;
-  SwcBC bc[2];
-};
-struct HaloArgs {
-  int dim;  // 0 x, 1 y, 2 z
-  int nf;
-  HaloField fld[SWC_MAX_FIELDS];
-  const void* rho;
-  int nx, ny, nz, h;
-  long long sx, sz;
-};
-
 template <typename T>
 __global__ void halo_kernel(const HaloArgs a) {
-  // Axis sizes with halos, storage order (z, x, y).
   const int ext[3] = {a.nx + 2 * a.h, a.ny + 2 * a.h, a.nz + 2 * a.h};
-  const long long stride[3] = {a.sx, 1, a.sz};
   const int d = a.dim;
-  // Plane axes (A, B) in storage order of the two other axes.
-  int ax_a, ax_b;
-  if (d == 0) { ax_a = 2; ax_b = 1; }
-  else if (d == 1) { ax_a = 2; ax_b = 0; }
-  else { ax_a = 0; ax_b = 1; }
-  const int na = ext[ax_a], nb = ext[ax_b];
-  const long long plane = (long long)na * nb;
+  const long long plane = (long long)ext[(d + 1) % 3] * ext[(d + 2) % 3];
   const long long total = plane * 2 * a.nf;
-  const int n = ext[d] - 2 * a.h;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-       t < total; t += (long long)gridDim.x * blockDim.x) {
-    const long long pb = t % plane;
-    const int side = (int)((t / plane) % 2);
-    const int fi = (int)(t / (plane * 2));
-    const int ia = (int)(pb / nb), ib = (int)(pb % nb);
-    const long long base = ia * stride[ax_a] + ib * stride[ax_b];
-    const long long sd = stride[d];
-    T* f = static_cast<T*>(a.fld[fi].f);
-    const T* rho = static_cast<const T*>(a.rho);
-    const bool prim = a.fld[fi].via_prim != 0;
-    const SwcBC bc = a.fld[fi].bc[side];
-    auto pv = [&](long long o) -> T {  // value the BC acts on
-      if (!prim) return f[o];
-      T r = rho[o];
-      return r == T(0) ? T(0) : f[o] / r;
-    };
-    auto put = [&](long long o, T val) { f[o] = prim ? rho[o] * val : val; };
-    if (bc.kind == SWC_BC_PERIODIC) {
-      for (int l = 0; l < a.h; ++l) {
-        if (side == 0) put(base + l * sd, pv(base + (long long)(l + n) * sd));
-        else put(base + (long long)(n + a.h + l) * sd, pv(base + (long long)(a.h + l) * sd));
-      }
-    } else if (bc.kind == SWC_BC_DIRICHLET) {
-      const T* pl = static_cast<const T*>(bc.planes);
-      for (int l = 0; l < a.h; ++l) {
-        T val = bc.per_layer ? pl[l * plane + pb] : T(bc.value);
-        long long o = side == 0 ? base + l * sd : base + (long long)(n + a.h + l) * sd;
-        put(o, val);
-      }
-    } else if (bc.kind == SWC_BC_NEUMANN) {
-      const T inc = T(bc.value);
-      if (side == 0) {
-        T v = pv(base + (long long)a.h * sd);
-        for (int l = 0; l < a.h; ++l) {
-          v = v - inc;
-          put(base + (long long)(a.h - 1 - l) * sd, v);
-        }
-      } else {
-        T v = pv(base + (long long)(n + a.h - 1) * sd);
-        for (int l = 0; l < a.h; ++l) {
-          v = v + inc;
-          put(base + (long long)(n + a.h + l) * sd, v);
-        }
-      }
-    }
-  }
+       t < total; t += (long long)gridDim.x * blockDim.x)
+    halo_elem<T>(a, t);
 }
 
 
@@ -203,19 +137,9 @@ __global__ void cfl_kernel(const CflArgs a) {
   }
 }
 
-__global__ void clock_begin_kernel(SwcClock* c) {
-  if (c->cfl > 0.0) {
-    double dt = c->cfl * c->dtmin;
-    if (c->t_end > 0.0) dt = fmin(dt, c->t_end - c->t);
-    c->dt = dt;
-  }
-  c->dtmin = 1e300;
-}
+__global__ void clock_begin_kernel(SwcClock* c) { clock_begin(c); }
 
-__global__ void clock_end_kernel(SwcClock* c) {
-  c->t += c->dt;
-  c->step += 1;
-}
+__global__ void clock_end_kernel(SwcClock* c) { clock_end(c); }
 
 // ---------------------------------------------------------------------------
 // Unit-level kernels.

@@ -13,7 +13,11 @@ namespace swc {
 #define SWC_DECL_STAGE(SUFFIX)                                               \
   int launch_stage_##SUFFIX(const StageArgs& a, int riemann, int visc,       \
                             int tile, cudaStream_t st);                      \
-  size_t stage_smem_##SUFFIX(int visc, int tile);
+  int launch_stage_batch_##SUFFIX(const StageBatch& b, int nblocks,          \
+                                  int riemann, int visc, int tile,           \
+                                  cudaStream_t st);                          \
+  size_t stage_smem_##SUFFIX(int visc, int tile);                          \
+  size_t stage_batch_smem_##SUFFIX(int visc, int tile);
 SWC_DECL_STAGE(f32_s0)
 SWC_DECL_STAGE(f32_s1)
 SWC_DECL_STAGE(f32_s2)
@@ -39,5 +43,22 @@ void note_launch(int n = 1);
 
 // Sets the message swc_last_error() reports on this thread; returns `code`.
 int record_error(int code, const char* fmt, ...);
+
+// SWC_OK, or SWC_ERR_ARG with the message set, for a grid's sizes/strides.
+int check_grid(const SwcGrid* g);
+
+// Device clock updates (SwcClock): start and end of a time step.
+__device__ __forceinline__ void clock_begin(SwcClock* c) {
+  if (c->cfl > 0.0) {
+    double dt = c->cfl * c->dtmin;
+    if (c->t_end > 0.0) dt = fmin(dt, c->t_end - c->t);
+    c->dt = dt;
+  }
+  c->dtmin = 1e300;
+}
+__device__ __forceinline__ void clock_end(SwcClock* c) {
+  c->t += c->dt;
+  c->step += 1;
+}
 
 }  // namespace swc

@@ -19,6 +19,9 @@
 #include "swc_physics.cuh"
 #include "swirlc_b200.h"
 
+// Members per batched launch (the member table is a launch parameter).
+#define SWC_BATCH_CHUNK 64
+
 namespace swc {
 
 struct StageArgs {
@@ -112,9 +115,10 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// One CTA's work: the TY x TX column at (y0, x0), z segment zb of `a`.
 template <typename T, int SCHEME, int RIEMANN, bool VISC, int TY, int TX>
-__global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
-    stage_kernel(const StageArgs a) {
+__device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
+                                           const int x0, const int zb) {
   using G = Geom<SCHEME, VISC>;
   using L = Layout<T, SCHEME, VISC, TY, TX>;
   constexpr int LO = G::LO, NW = G::NW, HR = G::HR, ZLO = G::ZLO,
@@ -141,8 +145,7 @@ __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
     ty = tid % TY;
     tx = tid / TY;
   }
-  const int y0 = blockIdx.x * TY, x0 = blockIdx.y * TX;
-  const int z0 = blockIdx.z * a.zseg;
+  const int z0 = zb * a.zseg;
   const int z1 = min(z0 + a.zseg, a.nz);
   const int h = a.halo;
   const int nxa = a.nx + 2 * h, nya = a.ny + 2 * h;
@@ -344,13 +347,14 @@ __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
   const int xa_c = x0 + tx + h, ya_c = y0 + ty + h;
 
   // Per plane every owner computes three faces of its cell (z above, y and
-  // x below); the last warp also computes the tile's high x-row and high
-  // y-column faces (TX + TY of them); owners of the last interior cell of a
-  // partial tile add the face beyond it.
-  const int wb = tid - (NT - 32);
+  // x below); the last TY + TX threads also compute the tile's high x-row
+  // and high y-column faces; owners of the last interior cell of a partial
+  // tile add the face beyond it.
+  static_assert(TY + TX <= NT, "boundary faces need TY + TX threads");
+  const int wb = tid - (NT - (TY + TX));
   int nj = own ? 3 : 0;
   int bkind = -1, bx = 0, by = 0;
-  if (wb >= 0 && wb < TY + TX) {
+  if (wb >= 0) {
     if (wb < TY) { bkind = 0; bx = TX; by = wb; }
     else { bkind = 1; bx = wb - TY; by = TY; }
     if (bkind == 0 && !(x0 + TX <= a.nx && y0 + by < a.ny)) bkind = -1;
@@ -464,6 +468,52 @@ __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
       if (tid == 0 && m < 1e300) atomic_min_pos(a.dtmin_out, m);
     }
   }
+}
+
+template <typename T, int SCHEME, int RIEMANN, bool VISC, int TY, int TX>
+__global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
+    stage_kernel(const StageArgs a) {
+  stage_body<T, SCHEME, RIEMANN, VISC, TY, TX>(a, blockIdx.x * TY,
+                                               blockIdx.y * TX, blockIdx.z);
+}
+
+// Batched stage: the CTAs of up to SWC_BATCH_CHUNK independent grids in one
+// launch. CTA t belongs to the member m with pre[m] <= t < pre[m+1]; its
+// tiles are numbered y fastest, then x, then z segment. The member table
+// travels in the launch parameters, so the launch needs no device memory
+// of its own and is captured whole by a CUDA graph.
+struct StageBatch {
+  int n;
+  int pre[SWC_BATCH_CHUNK + 1];
+  StageArgs m[SWC_BATCH_CHUNK];
+};
+
+template <typename T, int SCHEME, int RIEMANN, bool VISC, int TY, int TX>
+__global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
+    stage_batch_kernel(const StageBatch b) {
+  const int t = blockIdx.x;
+  int lo = 0, hi = b.n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (b.pre[mid] <= t) lo = mid;
+    else hi = mid;
+  }
+  // The member's record, copied to shared memory once per CTA, is read at
+  // fixed addresses (no register holds a per-member offset).
+  static_assert(sizeof(StageArgs) % 8 == 0, "StageArgs is copied as words");
+  __shared__ StageArgs sa;
+  {
+    const long long* src = reinterpret_cast<const long long*>(&b.m[lo]);
+    long long* dst = reinterpret_cast<long long*>(&sa);
+    for (int i = threadIdx.x; i < (int)(sizeof(StageArgs) / 8); i += blockDim.x)
+      dst[i] = src[i];
+  }
+  __syncthreads();
+  const int local = t - b.pre[lo];
+  const int nby = (sa.ny + TY - 1) / TY, nbx = (sa.nx + TX - 1) / TX;
+  const int by = local % nby, rest = local / nby;
+  stage_body<T, SCHEME, RIEMANN, VISC, TY, TX>(sa, by * TY, (rest % nbx) * TX,
+                                               rest / nbx);
 }
 
 }  // namespace swc

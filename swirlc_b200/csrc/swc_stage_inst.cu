@@ -54,6 +54,33 @@ int launch_rm(const StageArgs& a, int tile, cudaStream_t st) {
 #endif
 }
 
+// Batched launch of `nblocks` CTAs over the members of `b`. Tiles: 1 = 16x16
+// (y x x), 2 = 8x32 for members with ny <= 8.
+template <typename T, int RM, bool V, int TY, int TX>
+int launch_batch_tile(const StageBatch& b, int nblocks, cudaStream_t st) {
+  using Lay = Layout<T, SWC_SCHEME, V, TY, TX>;
+  auto kern = stage_batch_kernel<T, SWC_SCHEME, RM, V, TY, TX>;
+  static int attr_set = 0;
+  cudaError_t e;
+  if (!attr_set) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Lay::SMEM);
+    if (e != cudaSuccess) return SWC_ERR_LAUNCH;
+    attr_set = 1;
+  }
+  kern<<<nblocks, TY * TX, Lay::SMEM, st>>>(b);
+  note_launch();
+  e = cudaGetLastError();
+  return e == cudaSuccess ? SWC_OK : SWC_ERR_LAUNCH;
+}
+
+template <typename T, int RM, bool V>
+int launch_batch_rm(const StageBatch& b, int nblocks, int tile,
+                    cudaStream_t st) {
+  if (tile == 2) return launch_batch_tile<T, RM, V, 8, 32>(b, nblocks, st);
+  return launch_batch_tile<T, RM, V, 16, 16>(b, nblocks, st);
+}
+
 template <typename T, bool V>
 size_t smem_tile(int tile) {
 #if SWC_MULTI_TILE
@@ -78,6 +105,26 @@ int SWC_CAT(launch_stage_, SWC_SUFFIX)(const StageArgs& a, int riemann,
                 : launch_rm<T, 0, false>(a, tile, st);
   return visc ? launch_rm<T, 1, true>(a, tile, st)
               : launch_rm<T, 1, false>(a, tile, st);
+}
+
+int SWC_CAT(launch_stage_batch_, SWC_SUFFIX)(const StageBatch& b, int nblocks,
+                                             int riemann, int visc, int tile,
+                                             cudaStream_t st) {
+  using T = SWC_T;
+  if (riemann == SWC_HLL)
+    return visc ? launch_batch_rm<T, 0, true>(b, nblocks, tile, st)
+                : launch_batch_rm<T, 0, false>(b, nblocks, tile, st);
+  return visc ? launch_batch_rm<T, 1, true>(b, nblocks, tile, st)
+              : launch_batch_rm<T, 1, false>(b, nblocks, tile, st);
+}
+
+size_t SWC_CAT(stage_batch_smem_, SWC_SUFFIX)(int visc, int tile) {
+  using T = SWC_T;
+  if (tile == 2)
+    return visc ? Layout<T, SWC_SCHEME, true, 8, 32>::SMEM
+                : Layout<T, SWC_SCHEME, false, 8, 32>::SMEM;
+  return visc ? Layout<T, SWC_SCHEME, true, 16, 16>::SMEM
+              : Layout<T, SWC_SCHEME, false, 16, 16>::SMEM;
 }
 
 size_t SWC_CAT(stage_smem_, SWC_SUFFIX)(int visc, int tile) {

@@ -51,6 +51,8 @@ def test_argument_errors_need_no_gpu(lib):
     nat.check(lib.swc_clock_begin_step(None, None))
   with pytest.raises(ValueError):
     nat.check(lib.swc_rk_step_noalloc(None, None, None, 3, None, None, None))
+  with pytest.raises(ValueError):
+    nat.check(lib.swc_batch_step(None, 3, 1, None, None))
 
 
 def test_noalloc_limit_matches_header():
@@ -72,9 +74,13 @@ int main(void) {
   printf("SwcBC %zu\n", sizeof(SwcBC));
   printf("SwcFieldBC %zu\n", sizeof(SwcFieldBC));
   printf("SwcClock %zu\n", sizeof(SwcClock));
+  printf("SwcBatchMember %zu\n", sizeof(SwcBatchMember));
   F(SwcGrid, sx) F(SwcGrid, dz) F(SwcScheme, nu) F(SwcScheme, g)
   F(SwcScheme, pe_axis) F(SwcScheme, zseg) F(SwcBC, value) F(SwcBC, planes)
   F(SwcFieldBC, side) F(SwcClock, step)
+  F(SwcBatchMember, u) F(SwcBatchMember, work) F(SwcBatchMember, pe_axis)
+  F(SwcBatchMember, bcs) F(SwcBatchMember, clock) F(SwcBatchMember, tile)
+  F(SwcBatchMember, zseg)
   return 0;
 }
 '''
@@ -96,6 +102,7 @@ def test_struct_layouts_match_header():
   assert c['SwcBC'] == ctypes.sizeof(nat.SwcBC)
   assert c['SwcFieldBC'] == ctypes.sizeof(nat.SwcFieldBC)
   assert c['SwcClock'] == ctypes.sizeof(nat.SwcClock)
+  assert c['SwcBatchMember'] == ctypes.sizeof(nat.SwcBatchMember)
   for key, off in c.items():
     if '.' not in key:
       continue
