@@ -5,8 +5,11 @@ fill halos with the swc_halo_fill kernel: dims in order x, y, z, PERIODIC
 wrap, DIRICHLET scalar or per-layer planes, NEUMANN layer-by-layer
 extrapolation, and BCs given on a primitive applied to field/rho and
 multiplied back by the updated rho (boundary.py:34-86, 464-539, 606-629).
-Single replica; inter-replica halos come from the distributed exchange
-(swirlc_b200/parallel.py).
+With more than one replica (the grid split into cx x cy x cz blocks, one
+per process, rank = replica id), sides shared with another replica receive
+its interior layers through `halo_exchange.DistExchange` (torch.distributed),
+dim by dim; per-layer Dirichlet planes are then given per replica, as the
+reference expects them.
 """
 
 import ctypes
@@ -47,15 +50,53 @@ def _fill(fields, specs, vias, width: int, rho_index: int = -1):
   del keep
 
 
+def _periodic_of(specs):
+  out = []
+  for d in types.DIMS:
+    kinds = {bool(spec and spec.get(d)) and any(
+        bc_types.bc_value(v[0]) == 0 for v in spec[d].values())
+             for spec in specs}
+    if len(kinds) != 1:
+      raise NotImplementedError(
+          f'Fields disagree on whether dim {d} is periodic across replicas.')
+    out.append(kinds.pop())
+  return out
+
+
+def _fill_replicas(replica_id, replicas, fields, specs, vias, width: int):
+  """Halo update of `fields` (rho first when any BC is on a primitive) of
+  this replica: BCs on its outer sides, neighbours' layers on the others."""
+  from swirlc_b200 import halo_exchange as hx
+  import types as pytypes
+  t0 = fields[0]
+  grid = _grid_for(t0, width)
+  arr = (nat.SwcFieldBC * len(fields))()
+  keep = []
+  for i, (spec, via) in enumerate(zip(specs, vias)):
+    keep += engine.fill_field_bc(arr[i], spec, via, t0.shape, width, t0.dtype,
+                                 t0.device)
+  layout = hx.BlockLayout(np.asarray(replicas), _periodic_of(specs))
+  masked = hx.masked_bcs(pytypes.SimpleNamespace(bcs=arr), layout,
+                         int(replica_id), nat)
+
+  def bc_fill(rid, fs, dim):
+    nat.check(nat.load().swc_halo_fill(
+        ctypes.byref(grid), nat.dtype_code(t0.dtype), len(fs),
+        nat.ptr_array(fs), masked[dim], 0, nat.stream_ptr()), 'halo fill')
+
+  hx.DistExchange(layout, width, bc_fill, vias).fill([fields],
+                                                     [int(replica_id)])
+  del keep
+
+
 def exchange_halos(replica_id, replicas, u, bc_dict, width: int):
   """boundary.py:34-86 for one field; returns a new, halo-filled field."""
-  del replica_id
-  if np.asarray(replicas).size != 1:
-    raise NotImplementedError(
-        'Multi-replica halo exchange goes through swirlc_b200.parallel.')
   t = utils.as_tensor3d(u).contiguous().clone()
   if width > 0:
-    _fill([t], [bc_dict], [0], width)
+    if np.asarray(replicas).size != 1:
+      _fill_replicas(replica_id, replicas, [t], [bc_dict], [0], width)
+    else:
+      _fill([t], [bc_dict], [0], width)
   return utils.like_input(t, u)
 
 
@@ -68,9 +109,6 @@ def update_boundary(replica_id, replicas, states: Dict, cfg) -> Dict:
 def update_conservative_cell_averages(replica_id, replicas, conservative,
                                       cfg) -> Dict:
   """boundary.py:464-539: halo fill of every conserved variable."""
-  if np.asarray(replicas).size != 1:
-    raise NotImplementedError(
-        'Multi-replica halo exchange goes through swirlc_b200.parallel.')
   bc = cfg.bc[_CELL_AVG_BC]
   names = list(conservative.keys())
   specs, vias = [], []
@@ -93,7 +131,14 @@ def update_conservative_cell_averages(replica_id, replicas, conservative,
   # rho first so primitive BCs see its final halos (boundary.py:484-487).
   order = ([rho_index] if rho_index >= 0 else []) + [
       i for i in range(len(names)) if i != rho_index]
-  if cfg.halo_width > 0:
+  if cfg.halo_width > 0 and np.asarray(replicas).size != 1:
+    if len(order) > nat.SWC_MAX_FIELDS:
+      raise NotImplementedError(
+          f'At most {nat.SWC_MAX_FIELDS} fields per multi-replica halo update.')
+    _fill_replicas(replica_id, replicas, [fields[i] for i in order],
+                   [specs[i] for i in order], [vias[i] for i in order],
+                   cfg.halo_width)
+  elif cfg.halo_width > 0:
     for lo in range(0, len(order), nat.SWC_MAX_FIELDS):
       chunk = order[lo:lo + nat.SWC_MAX_FIELDS]
       if rho_index >= 0 and rho_index not in chunk and any(vias[i] for i in chunk):

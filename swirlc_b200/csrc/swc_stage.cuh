@@ -321,24 +321,18 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
     }
   };
 
-  // ---- warm-up: planes zfirst .. z0+ZHI-1 through the staging buffer.
-  for (int i = 0; i < RING; ++i) {
+  // ---- warm-up: planes zfirst .. z0+ZHI-2 through the staging buffer; the
+  // loop's first pass (zc = z0-1) adds plane z0+ZHI-1 and only computes the
+  // z-face below the segment, so that every face of every segment comes from
+  // the same code (results do not depend on where segments start).
+  for (int i = 0; i < RING - 1; ++i) {
     issue_plane(zfirst + i);
     cp_async_wait_all();
     convert_plane(zfirst + i, i);
   }
-  issue_plane(z0 + ZHI);  // first plane of the main loop, in flight
-  __syncthreads();
+  issue_plane(z0 + ZHI - 1);  // plane of the loop's first pass, in flight
   const bool own = (x0 + tx < a.nx) && (y0 + ty < a.ny);
   T flo[5];
-  if (own) {
-    do_face(2, z0 - 1, tx, ty);
-#pragma unroll
-    for (int v = 0; v < 5; ++v) flo[v] = fz[(v * TX + tx) * TY + ty];
-  }
-  // The first loop iteration overwrites the slot of plane z0-ZLO-1, which the
-  // z-face above reads, and the z-flux buffer.
-  __syncthreads();
 
   double dtmin_local = 1e300;
   const double dt_d = a.dt ? *a.dt : 0.0;
@@ -363,7 +357,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
   const bool ex_x = own && (x0 + tx + 1 == a.nx) && (tx + 1 < TX);
   const bool ex_y = own && (y0 + ty + 1 == a.ny) && (ty + 1 < TY);
 
-  for (int zc = z0; zc < z1; ++zc) {
+  for (int zc = z0 - 1; zc < z1; ++zc) {
     // The plane zc+ZHI (staged during the previous plane) replaces the slot
     // of plane zc-ZLO-1, last read before the barrier that ended the
     // previous iteration.
@@ -372,7 +366,8 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
     __syncthreads();
     if (zc + 1 < z1) issue_plane(zc + ZHI + 1);
 
-    const int ntot = nj + (bkind >= 0) + ex_x + ex_y;
+    const bool pre = zc < z0;  // only the z-face below the segment
+    const int ntot = pre ? (own ? 1 : 0) : nj + (bkind >= 0) + ex_x + ex_y;
     for (int j = 0; j < ntot; ++j) {
       int kind, fxx, fyy;
       if (j < nj) {
@@ -392,6 +387,13 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
       do_face(kind, zc, fxx, fyy);
     }
     __syncthreads();
+    if (pre) {
+      if (own) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) flo[v] = fz[(v * TX + tx) * TY + ty];
+      }
+      continue;
+    }
 
     // ---- divergence, source and stage combination.
     if (own) {

@@ -1,0 +1,173 @@
+"""Time loop of a grid decomposed into blocks (the reference's replicas).
+
+The global grid of `cfg` (cfg.x, cfg.y, cfg.z; `halo_width` layers) is split
+into cx x cy x cz blocks as in the reference (utils.py:24-40,
+simulation.py:53-56). Each block runs the same fused stage kernels as a
+single grid; before every stage its halos are updated by a
+`halo_exchange` transport (neighbour blocks' interior layers on inner sides,
+boundary conditions on the others), and after the last stage of a step the
+CFL limit is min-reduced over all blocks, so every block takes the same dt.
+A decomposed run reproduces the single-grid run bit for bit: the
+`mesh_local` halo-coordinate rule (utils.py:58-89) gives an inner block's
+halo cells its neighbours' coordinates.
+"""
+
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from swirlc_b200 import _native as nat
+from swirlc_b200 import engine
+from swirlc_b200 import halo_exchange as hx
+from swirlc_b200.common import types
+from swirlc_b200.core import parameter
+from swirlc_b200.physics import physics_models as pm_lib
+
+_CELL_AVG = 'cell_averages'
+periodic_dims = hx.periodic_dims
+localize_bc = hx.localize_bc
+
+
+def split_state(state: Dict[str, np.ndarray], replicas: np.ndarray,
+                hw: int) -> Dict[int, Dict[str, np.ndarray]]:
+  """Cuts a global state with halos into the blocks of `replicas`, each with
+  its own halo layers (values there are overwritten by the first fill)."""
+  cx, cy, cz = replicas.shape
+  out = {}
+  for (i, j, k), rid in np.ndenumerate(replicas):
+    blk = {}
+    for name, a in state.items():
+      nz, nx, ny = (s - 2 * hw for s in a.shape)
+      lz, lx, ly = nz // cz, nx // cx, ny // cy
+      blk[name] = np.ascontiguousarray(
+          a[k * lz:k * lz + lz + 2 * hw, i * lx:i * lx + lx + 2 * hw,
+            j * ly:j * ly + ly + 2 * hw])
+    out[int(rid)] = blk
+  return out
+
+
+def join_interiors(blocks: Dict[int, Dict[str, np.ndarray]],
+                   replicas: np.ndarray, hw: int) -> Dict[str, np.ndarray]:
+  """Global interior (no halos) assembled from the blocks' interiors."""
+  names = list(next(iter(blocks.values())).keys())
+  out = {}
+  for name in names:
+    rows = []
+    for k in range(replicas.shape[2]):
+      cols = []
+      for i in range(replicas.shape[0]):
+        segs = [blocks[int(replicas[i, j, k])][name][hw:-hw, hw:-hw, hw:-hw]
+                for j in range(replicas.shape[1])]
+        cols.append(np.concatenate(segs, axis=2))
+      rows.append(np.concatenate(cols, axis=1))
+    out[name] = np.concatenate(rows, axis=0)
+  return out
+
+
+class DecomposedStepper:
+  """RK3/RK2 steps of the blocks `rids` of a decomposed grid.
+
+  Args:
+    cfg: user config dict or `SwirlCParameters` of the global grid, with
+      cx, cy, cz blocks.
+    states: {replica id: state dict} of the blocks held by this process,
+      each (nz/cz + 2h, nx/cx + 2h, ny/cy + 2h).
+    transport: 'local' (all blocks in this process) or 'dist' (this
+      process's single block; peers over torch.distributed, rank = id).
+    dt, cfl, t_end, scheme: as `engine.Stepper`.
+  """
+
+  def __init__(self, cfg, states: Dict[int, Dict], dtype=torch.float32,
+               transport: str = 'local', dt: Optional[float] = None,
+               cfl: Optional[float] = None, t_end: Optional[float] = None,
+               scheme: str = 'rk3', device=None):
+    if not isinstance(cfg, parameter.SwirlCParameters):
+      cfg = parameter.SwirlCParameters(cfg)
+    if scheme not in ('rk3', 'rk2'):
+      raise NotImplementedError(f'"{scheme}" is not implemented as an '
+                                '"time_integration_scheme".')
+    self.cfg = cfg
+    self.order = 3 if scheme == 'rk3' else 2
+    shape = (cfg.cx, cfg.cy, cfg.cz)
+    self.replicas = np.arange(int(np.prod(shape)), dtype=np.int32).reshape(shape)
+    self.layout = hx.BlockLayout(self.replicas, periodic_dims(cfg))
+    self.rids = sorted(int(r) for r in states)
+    if transport == 'local' and len(self.rids) != self.layout.n_blocks:
+      raise ValueError('The local transport needs every block in this process.')
+    if transport == 'dist' and len(self.rids) != 1:
+      raise ValueError('The distributed transport holds one block per process.')
+    self.hw = int(cfg.halo_width)
+    pm = pm_lib.PhysicsModels(cfg)
+    self.solvers: List[engine.Solver] = []
+    self.u: List[List[torch.Tensor]] = []
+    self.w1: List[List[torch.Tensor]] = []
+    self.w2: List[List[torch.Tensor]] = []
+    self.clocks: List[torch.Tensor] = []
+    dev = device or torch.device('cuda', torch.cuda.current_device())
+    for rid in self.rids:
+      st = states[rid]
+      f = [torch.as_tensor(st[k]).to(device=dev, dtype=dtype).contiguous()
+           for k in types.BASE_CONSERVATIVE]
+      s = engine.Solver(cfg, pm, f[0].shape, dtype, dev, replica_id=rid,
+                        replicas=self.replicas)
+      s.check_fields(f)
+      self.solvers.append(s)
+      self.u.append(f)
+      self.w1.append(s.new_fields(zero=False))
+      self.w2.append(s.new_fields(zero=False))
+    via = [self.solvers[0].bcs[i].via_primitive for i in range(5)]
+    index = {rid: i for i, rid in enumerate(self.rids)}
+
+    def bc_fill(rid, fields, dim):
+      self.solvers[index[rid]].fill_boundary_dim(fields, dim)
+
+    cls = hx.LocalExchange if transport == 'local' else hx.DistExchange
+    self.exchange = cls(self.layout, self.hw, bc_fill, via)
+    mdt = float(cfg.dt if dt is None else dt)
+    mcfl = float((getattr(cfg, 'cfl', 0.0) or 0.0) if cfl is None else cfl)
+    mend = float((getattr(cfg, 't_end', 0.0) or 0.0) if t_end is None
+                 else t_end)
+    for s, f in zip(self.solvers, self.u):
+      c = torch.zeros(6, dtype=torch.float64, device=dev)
+      c[1], c[2], c[3], c[4] = mdt, 1e300, mcfl, mend
+      if mcfl > 0.0:
+        s.cfl_reduce(f, c[2:3])
+      self.clocks.append(c)
+    if mcfl > 0.0:
+      self.exchange.min_all([c[2:3] for c in self.clocks])
+
+  def _stage(self, uk, u0, out, mode, c0=0.0, c1=0.0, reduce=False):
+    for i, s in enumerate(self.solvers):
+      s.stage(uk[i], None if u0 is None else u0[i], out[i], mode, c0, c1,
+              dt=self.clocks[i][1:2],
+              dtmin_out=self.clocks[i][2:3] if reduce else None)
+
+  def step(self, n: int = 1) -> None:
+    lib = nat.load()
+    for _ in range(n):
+      for c in self.clocks:
+        nat.check(lib.swc_clock_begin_step(c.data_ptr(), nat.stream_ptr()))
+      self.exchange.fill(self.u, self.rids)
+      self._stage(self.u, None, self.w1, nat.SWC_OUT_EULER)
+      self.exchange.fill(self.w1, self.rids)
+      if self.order == 3:
+        self._stage(self.w1, self.u, self.w2, nat.SWC_OUT_CONVEX, 0.75, 0.25)
+        self.exchange.fill(self.w2, self.rids)
+        self._stage(self.w2, self.u, self.u, nat.SWC_OUT_CONVEX, 1.0 / 3.0,
+                    2.0 / 3.0, reduce=True)
+      else:
+        self._stage(self.w1, self.u, self.u, nat.SWC_OUT_AVERAGE, 0.5, 0.0,
+                    reduce=True)
+      self.exchange.min_all([c[2:3] for c in self.clocks])
+      for c in self.clocks:
+        nat.check(lib.swc_clock_end_step(c.data_ptr(), nat.stream_ptr()))
+
+  def states(self) -> Dict[int, Dict[str, np.ndarray]]:
+    torch.cuda.synchronize()
+    return {rid: {k: f.cpu().numpy() for k, f in
+                  zip(types.BASE_CONSERVATIVE, u)}
+            for rid, u in zip(self.rids, self.u)}
+
+  def time(self) -> float:
+    return float(self.clocks[0][0].item())

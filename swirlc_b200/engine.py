@@ -196,12 +196,27 @@ class Solver:
           self._pe[i] = a.to(self.device).contiguous()
           sc.pe_axis[i] = self._pe[i].data_ptr()
     self.scheme = sc
+    self.replica_id = int(replica_id)
+    self.replicas = None if replicas is None else np.asarray(replicas)
+    self._layout = None
+    if self.replicas is not None and self.replicas.size > 1:
+      from swirlc_b200 import halo_exchange as hx
+      self._layout = hx.BlockLayout(self.replicas, hx.periodic_dims(cfg))
+      glob = tuple(np.asarray(getattr(cfg, d)).shape[0] for d in ('z', 'x', 'y'))
+      self._bc_cells = hx.localize_bc(cfg.bc.get(_CELL_AVG, {}), self.replicas,
+                                      self.replica_id, hw, glob)
+    else:
+      self._bc_cells = cfg.bc.get(_CELL_AVG, {})
     self._build_bcs()
+    self._masked = None
+    self._exchange = None
+    if self._layout is not None:
+      self._masked = hx.masked_bcs(self, self._layout, self.replica_id, nat)
     self._dt_cache: Dict[float, torch.Tensor] = {}
 
   # ------------------------------------------------------------------ BCs
   def _build_bcs(self):
-    bc_all = self.cfg.bc.get(_CELL_AVG, {})
+    bc_all = self._bc_cells
     self._planes = []
     arr = (nat.SwcFieldBC * len(self.names))()
     for fi, name in enumerate(self.names):
@@ -239,11 +254,35 @@ class Solver:
     return t
 
   def fill_halos(self, fields: Sequence[torch.Tensor]) -> None:
-    """In-place halo fill (boundary.update_conservative_cell_averages)."""
+    """In-place halo fill (boundary.update_conservative_cell_averages). With
+    replicas > 1, halos on inner sides come from the neighbouring replicas
+    over torch.distributed (rank = replica id), the others from the BCs."""
+    if self._layout is not None:
+      if self._exchange is None:
+        from swirlc_b200 import halo_exchange as hx
+        via = [self.bcs[i].via_primitive for i in range(len(self.bcs))]
+        self._exchange = hx.DistExchange(
+            self._layout, self.hw,
+            lambda rid, fs, dim: self.fill_boundary_dim(fs, dim), via)
+      self._exchange.fill([list(fields)], [self.replica_id])
+      return
     ptrs = nat.ptr_array(fields)
     nat.check(nat.load().swc_halo_fill(
         ctypes.byref(self.grid), self.scheme.dtype, len(fields), ptrs,
         self.bcs, 0, nat.stream_ptr()), 'halo fill')
+
+  def fill_boundary_dim(self, fields: Sequence[torch.Tensor], dim: int) -> None:
+    """Halo fill along `dim` of the sides that take a boundary condition
+    (not the sides shared with another replica)."""
+    bcs = self._masked[dim] if self._masked is not None else None
+    if bcs is None:
+      from swirlc_b200 import halo_exchange as hx
+      layout = hx.BlockLayout(np.zeros((1, 1, 1), np.int32), [False] * 3)
+      self._masked = hx.masked_bcs(self, layout, 0, nat)
+      bcs = self._masked[dim]
+    nat.check(nat.load().swc_halo_fill(
+        ctypes.byref(self.grid), self.scheme.dtype, len(fields),
+        nat.ptr_array(fields), bcs, 0, nat.stream_ptr()), 'halo fill')
 
   def stage(self, uk, u0, uout, mode: int, c0: float = 0.0, c1: float = 0.0,
             dt: Optional[torch.Tensor] = None,
