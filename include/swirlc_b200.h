@@ -139,6 +139,55 @@ int swc_rk_stage(const SwcGrid* grid, const SwcScheme* scheme,
                  void* const* uout, int32_t mode, double c0, double c1,
                  const double* dt, double* dtmin_out, void* stream);
 
+/* Extensions of the fused stage: transported scalars, hydrostatic helper
+ * states and face / flux boundary conditions. */
+#define SWC_MAX_OVERRIDES 8
+/* Face BC (boundary.py:186-461): a primitive (u, v, w, e, phi) or its
+ * conservative (rho_u, ..., rho_phi) set on both face states. */
+enum { SWC_FACE_PRIMITIVE = 0, SWC_FACE_CONSERVATIVE = 1 };
+/* Flux BC type (bc_types.BoundaryFluxType; boundary.py:89-183). */
+enum { SWC_FLUX_CONVECTIVE = 0, SWC_FLUX_DIFFUSIVE = 1, SWC_FLUX_TOTAL = 2 };
+
+typedef struct SwcOverride {
+  int32_t var;        /* 1..3 velocity / momentum x, y, z; 4 e / rho_e;
+                         5 + k scalar k (flux BCs: 0 is rho as well)     */
+  int32_t mode;       /* face: SWC_FACE_*; flux: SWC_FLUX_*              */
+  double value;       /* used when `plane` is NULL                       */
+  const void* plane;  /* one face plane [A][B] in dtype, axes as in
+                         SwcBC.planes (halos included), or NULL          */
+} SwcOverride;
+
+typedef struct SwcStageExt {
+  /* Hydrostatic reference states (fields with halos), both or neither:
+   * the momentum flux and HLLC use p_dyn = p - p_ref, reconstructed like
+   * the primitives with p_dyn = 0 in the halos of outer sides, and gravity
+   * acts on rho - rho_ref (compressible_navier_stokes.py:299-335,
+   * hllc.py:105-120). HLLC takes its sound speeds from p_dyn, as the
+   * reference does, so p_dyn must stay >= 0 on the faces. */
+  const void* p_ref;
+  const void* rho_ref;
+  int32_t boundary[3][2]; /* 1: side [dim][low/high] is on the boundary of
+                             the whole grid (all sides for one grid)     */
+  int32_t nface[3][2];    /* face overrides per side                     */
+  int32_t nflux[3][2];    /* flux overrides per side                     */
+  int32_t reserved;
+  SwcOverride face[3][2][SWC_MAX_OVERRIDES];
+  SwcOverride flux[3][2][SWC_MAX_OVERRIDES];
+} SwcStageExt;
+
+/* swc_rk_stage with the extensions above. Fields: 5 + scheme->nscalars
+ * (rho_phi_k after rho_e). `ext` may be NULL (no helper states, no face or
+ * flux BCs). Face overrides act on the faces between the halo and the
+ * interior on sides marked `boundary`; a density face BC is not supported
+ * (in the reference it drops p and h from the face primitives). Face BCs
+ * with diffusion are rejected, as in the reference
+ * (compressible_navier_stokes.py:185-196). */
+int swc_rk_stage_ext(const SwcGrid* grid, const SwcScheme* scheme,
+                     const SwcStageExt* ext, const void* const* uk,
+                     const void* const* u0, void* const* uout, int32_t mode,
+                     double c0, double c1, const double* dt,
+                     double* dtmin_out, void* stream);
+
 /* One time step in place on `u` (5 fields): [clock begin] -> halo fill ->
  * fused stages -> [clock end]. order 3: SSP-RK3 (rk3.py:87-120); order 2:
  * RK2 (rk2.py:69-86). `work` holds 10 field buffers (two states of the

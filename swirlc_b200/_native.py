@@ -40,7 +40,7 @@ EXPORTED = (
     'swc_rk_stage', 'swc_cfl_reduce', 'swc_clock_begin_step',
     'swc_clock_end_step', 'swc_reconstruct', 'swc_riemann_flux',
     'swc_wave_speeds', 'swc_stencil', 'swc_rk_combine', 'swc_rk_step',
-    'swc_rk_step_noalloc', 'swc_batch_step',
+    'swc_rk_step_noalloc', 'swc_batch_step', 'swc_rk_stage_ext',
 )
 
 # Built-in work space of swc_rk_step_noalloc (SWC_NOALLOC_MAX_BYTES).
@@ -79,6 +79,26 @@ class SwcClock(ctypes.Structure):
   _fields_ = [('t', ctypes.c_double), ('dt', ctypes.c_double),
               ('dtmin', ctypes.c_double), ('cfl', ctypes.c_double),
               ('t_end', ctypes.c_double), ('step', ctypes.c_int64)]
+
+
+SWC_MAX_OVERRIDES = 8
+SWC_FACE_PRIMITIVE, SWC_FACE_CONSERVATIVE = 0, 1
+SWC_FLUX_CONVECTIVE, SWC_FLUX_DIFFUSIVE, SWC_FLUX_TOTAL = 0, 1, 2
+
+
+class SwcOverride(ctypes.Structure):
+  _fields_ = [('var', ctypes.c_int32), ('mode', ctypes.c_int32),
+              ('value', ctypes.c_double), ('plane', ctypes.c_void_p)]
+
+
+class SwcStageExt(ctypes.Structure):
+  _fields_ = [('p_ref', ctypes.c_void_p), ('rho_ref', ctypes.c_void_p),
+              ('boundary', (ctypes.c_int32 * 2) * 3),
+              ('nface', (ctypes.c_int32 * 2) * 3),
+              ('nflux', (ctypes.c_int32 * 2) * 3),
+              ('reserved', ctypes.c_int32),
+              ('face', ((SwcOverride * SWC_MAX_OVERRIDES) * 2) * 3),
+              ('flux', ((SwcOverride * SWC_MAX_OVERRIDES) * 2) * 3)]
 
 
 class SwcBatchMember(ctypes.Structure):
@@ -137,6 +157,10 @@ def load(require_cuda: bool = True) -> ctypes.CDLL:
                                   ctypes.POINTER(SwcScheme),
                                   ctypes.POINTER(SwcFieldBC), i32, pp, pp, vp,
                                   vp]
+      lib.swc_rk_stage_ext.argtypes = [ctypes.POINTER(SwcGrid),
+                                       ctypes.POINTER(SwcScheme),
+                                       ctypes.POINTER(SwcStageExt), pp, pp, pp,
+                                       i32, dbl, dbl, vp, vp, vp]
       lib.swc_batch_step.argtypes = [ctypes.POINTER(SwcScheme), i32, i32,
                                      ctypes.POINTER(SwcBatchMember), vp]
       lib.swc_rk_step_noalloc.argtypes = [ctypes.POINTER(SwcGrid),

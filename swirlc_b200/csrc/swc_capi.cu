@@ -229,43 +229,13 @@ __global__ void riemann_kernel(const PointArgs a) {
 #pragma unroll
     for (int k = 0; k < 5; ++k) static_cast<T*>(a.out[k])[i] = f[k];
     if (a.ns > 0) {
-      const T ml = l.r * l.u[D], mr = r.r * r.u[D];
-      if constexpr (RM == 0) {
-        T s_l, s_r;
-        hll_speeds<T, D>(l, r, pe, s_l, s_r);
-        T ds = s_r - s_l;
-        T t1 = dnn(min_(s_r, T(0)) - min_(s_l, T(0)), ds);
-        T t2 = T(1) - t1;
-        T t3 = dnn(s_r * abs_(s_l) - s_l * abs_(s_r), T(2) * ds);
-        for (int k = 0; k < a.ns; ++k) {
-          T pl = static_cast<const T*>(a.ql[7 + k])[i];
-          T pr = static_cast<const T*>(a.qr[7 + k])[i];
-          static_cast<T*>(a.out[5 + k])[i] =
-              t1 * (mr * pr) + t2 * (ml * pl) -
-              t3 * (mul_rn(r.r, pr) - mul_rn(l.r, pl));
-        }
-      } else {
-        Prim<T> lu = l, ru = r;
-        lu.p = pdl;
-        ru.p = pdr;
-        T s_l, s_r;
-        hll_speeds<T, D>(lu, ru, pe, s_l, s_r);
-        T s_m = hllc_contact<T, D>(lu, ru, s_l, s_r);
-        bool c1 = s_l >= T(0);
-        bool c2 = (s_l <= T(0)) && (s_m >= T(0));
-        bool c3 = (s_m <= T(0)) && (s_r >= T(0));
-        bool left = c1 || c2;
-        bool star = !c1 && (c2 || c3);
-        const Prim<T>& q = left ? l : r;
-        T s_k = left ? s_l : s_r;
-        T m = left ? ml : mr;
-        for (int k = 0; k < a.ns; ++k) {
-          T ph = static_cast<const T*>(left ? a.ql[7 + k] : a.qr[7 + k])[i];
-          T fk = m * ph;
-          if (star) fk = fk + q.r * (s_m - q.u[D]) * ph * dnn(s_k, s_k - s_m);
-          static_cast<T*>(a.out[5 + k])[i] = fk;
-        }
+      T phl[3], phr[3], fs[3];
+      for (int k = 0; k < a.ns; ++k) {
+        phl[k] = static_cast<const T*>(a.ql[7 + k])[i];
+        phr[k] = static_cast<const T*>(a.qr[7 + k])[i];
       }
+      scalar_fluxes<RM, T, D>(l, r, pdl, pdr, pe, a.ns, phl, phr, fs);
+      for (int k = 0; k < a.ns; ++k) static_cast<T*>(a.out[5 + k])[i] = fs[k];
     }
   }
 }
@@ -417,10 +387,12 @@ int swc_halo_fill(const SwcGrid* grid, int32_t dtype, int32_t nfields,
   return SWC_OK;
 }
 
-int swc_rk_stage(const SwcGrid* grid, const SwcScheme* sc,
-                 const void* const* uk, const void* const* u0,
-                 void* const* uout, int32_t mode, double c0, double c1,
-                 const double* dt, double* dtmin_out, void* stream) {
+// Checks and the kernel arguments shared by swc_rk_stage and
+// swc_rk_stage_ext; `nf` conserved fields (5 + scalars).
+static int stage_args(const SwcGrid* grid, const SwcScheme* sc, int nf,
+                      const void* const* uk, const void* const* u0,
+                      void* const* uout, int32_t mode, double c0, double c1,
+                      const double* dt, double* dtmin_out, StageArgs& a) {
   int st = check_grid(grid);
   if (st) return st;
   if (!sc) return fail(SWC_ERR_ARG, "scheme is NULL");
@@ -429,12 +401,10 @@ int swc_rk_stage(const SwcGrid* grid, const SwcScheme* sc,
     return fail(SWC_ERR_UNSUPPORTED, "interpolation scheme %d is not implemented", sc->interp);
   if (sc->riemann != SWC_HLL && sc->riemann != SWC_HLLC)
     return fail(SWC_ERR_ARG, "numeric flux scheme %d is not implemented", sc->riemann);
-  if (sc->nscalars != 0)
-    return fail(SWC_ERR_UNSUPPORTED, "transported scalars are not supported by the fused stage");
   if (mode < SWC_OUT_RHS || mode > SWC_OUT_AVERAGE)
     return fail(SWC_ERR_ARG, "bad stage mode %d", mode);
   if (!uk || !uout) return fail(SWC_ERR_ARG, "NULL field list");
-  for (int v = 0; v < 5; ++v) {
+  for (int v = 0; v < nf; ++v) {
     if (!uk[v] || !uout[v]) return fail(SWC_ERR_ARG, "NULL field %d", v);
     if (uout[v] == uk[v]) return fail(SWC_ERR_ARG, "uout must not alias uk");
     if ((mode == SWC_OUT_CONVEX || mode == SWC_OUT_AVERAGE) && (!u0 || !u0[v]))
@@ -446,12 +416,11 @@ int swc_rk_stage(const SwcGrid* grid, const SwcScheme* sc,
   if (grid->halo < need)
     return fail(SWC_ERR_ARG, "halo_width %d is too small for this scheme (needs %d)",
                 grid->halo, need);
-  StageArgs a;
   memset(&a, 0, sizeof(a));
   a.nx = grid->nx; a.ny = grid->ny; a.nz = grid->nz; a.halo = grid->halo;
   a.sx = grid->sx; a.sz = grid->sz;
   a.dx = grid->dx; a.dy = grid->dy; a.dz = grid->dz;
-  for (int v = 0; v < 5; ++v) {
+  for (int v = 0; v < nf; ++v) {
     a.uk[v] = uk[v];
     a.u0[v] = u0 ? u0[v] : nullptr;
     a.uout[v] = uout[v];
@@ -473,6 +442,20 @@ int swc_rk_stage(const SwcGrid* grid, const SwcScheme* sc,
     zseg = (int)std::max<long long>(8, (grid->nz + nseg - 1) / nseg);
   }
   a.zseg = std::min(zseg, grid->nz);
+  return SWC_OK;
+}
+
+int swc_rk_stage(const SwcGrid* grid, const SwcScheme* sc,
+                 const void* const* uk, const void* const* u0,
+                 void* const* uout, int32_t mode, double c0, double c1,
+                 const double* dt, double* dtmin_out, void* stream) {
+  if (sc && sc->nscalars != 0)
+    return fail(SWC_ERR_UNSUPPORTED,
+                "transported scalars go through swc_rk_stage_ext");
+  StageArgs a;
+  int st = stage_args(grid, sc, 5, uk, u0, uout, mode, c0, c1, dt, dtmin_out, a);
+  if (st) return st;
+  const int visc = sc->diffusion ? 1 : 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int tile = sc->tile;
   int rc;
@@ -489,6 +472,80 @@ int swc_rk_stage(const SwcGrid* grid, const SwcScheme* sc,
       case 1: rc = launch_stage_f64_s1(a, sc->riemann, visc, tile, s); break;
       case 2: rc = launch_stage_f64_s2(a, sc->riemann, visc, tile, s); break;
       default: rc = launch_stage_f64_s3(a, sc->riemann, visc, tile, s); break;
+    }
+  }
+  if (rc) return fail(rc, "stage launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  return SWC_OK;
+}
+
+int swc_rk_stage_ext(const SwcGrid* grid, const SwcScheme* sc,
+                     const SwcStageExt* ext, const void* const* uk,
+                     const void* const* u0, void* const* uout, int32_t mode,
+                     double c0, double c1, const double* dt,
+                     double* dtmin_out, void* stream) {
+  if (!sc) return fail(SWC_ERR_ARG, "scheme is NULL");
+  const int ns = sc->nscalars;
+  if (ns < 0 || ns > 3)
+    return fail(SWC_ERR_UNSUPPORTED, "%d transported scalars (at most 3)", ns);
+  SwcStageExt e;
+  memset(&e, 0, sizeof(e));
+  if (ext) {
+    e = *ext;
+  } else {
+    for (int d = 0; d < 3; ++d) e.boundary[d][0] = e.boundary[d][1] = 1;
+  }
+  if ((e.p_ref == nullptr) != (e.rho_ref == nullptr))
+    return fail(SWC_ERR_ARG, "p_ref and rho_ref go together");
+  bool any_face = false;
+  for (int d = 0; d < 3; ++d)
+    for (int sd = 0; sd < 2; ++sd) {
+      if (e.nface[d][sd] < 0 || e.nface[d][sd] > SWC_MAX_OVERRIDES ||
+          e.nflux[d][sd] < 0 || e.nflux[d][sd] > SWC_MAX_OVERRIDES)
+        return fail(SWC_ERR_ARG, "bad override count on side (%d, %d)", d, sd);
+      for (int i = 0; i < e.nface[d][sd]; ++i) {
+        const SwcOverride& o = e.face[d][sd][i];
+        if (o.var == 0)
+          return fail(SWC_ERR_UNSUPPORTED,
+                      "a density face boundary condition is not supported");
+        if (o.var < 1 || o.var > 4 + ns ||
+            (o.mode != SWC_FACE_PRIMITIVE && o.mode != SWC_FACE_CONSERVATIVE))
+          return fail(SWC_ERR_ARG, "bad face override (var %d, mode %d)", o.var,
+                      o.mode);
+        any_face = true;
+      }
+      for (int i = 0; i < e.nflux[d][sd]; ++i) {
+        const SwcOverride& o = e.flux[d][sd][i];
+        if (o.var < 0 || o.var > 4 + ns || o.mode < SWC_FLUX_CONVECTIVE ||
+            o.mode > SWC_FLUX_TOTAL)
+          return fail(SWC_ERR_ARG, "bad flux override (var %d, type %d)", o.var,
+                      o.mode);
+      }
+    }
+  if (any_face && sc->diffusion)
+    return fail(SWC_ERR_UNSUPPORTED,
+                "Face boundary conditions are not supported with diffusion "
+                "enabled at this time.");
+  StageArgs a;
+  int st = stage_args(grid, sc, 5 + ns, uk, u0, uout, mode, c0, c1, dt,
+                      dtmin_out, a);
+  if (st) return st;
+  const int visc = sc->diffusion ? 1 : 0;
+  const int help = e.p_ref ? 1 : 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc;
+  if (sc->dtype == SWC_F32) {
+    switch (sc->interp) {
+      case 0: rc = launch_stage_ext_f32_s0(a, e, sc->riemann, visc, ns, help, s); break;
+      case 1: rc = launch_stage_ext_f32_s1(a, e, sc->riemann, visc, ns, help, s); break;
+      case 2: rc = launch_stage_ext_f32_s2(a, e, sc->riemann, visc, ns, help, s); break;
+      default: rc = launch_stage_ext_f32_s3(a, e, sc->riemann, visc, ns, help, s); break;
+    }
+  } else {
+    switch (sc->interp) {
+      case 0: rc = launch_stage_ext_f64_s0(a, e, sc->riemann, visc, ns, help, s); break;
+      case 1: rc = launch_stage_ext_f64_s1(a, e, sc->riemann, visc, ns, help, s); break;
+      case 2: rc = launch_stage_ext_f64_s2(a, e, sc->riemann, visc, ns, help, s); break;
+      default: rc = launch_stage_ext_f64_s3(a, e, sc->riemann, visc, ns, help, s); break;
     }
   }
   if (rc) return fail(rc, "stage launch failed: %s", cudaGetErrorString(cudaGetLastError()));

@@ -16,6 +16,9 @@ namespace swc {
   int launch_stage_batch_##SUFFIX(const StageBatch& b, int nblocks,          \
                                   int riemann, int visc, int tile,           \
                                   cudaStream_t st);                          \
+  int launch_stage_ext_##SUFFIX(const StageArgs& a, const SwcStageExt& e,   \
+                                int riemann, int visc, int ns, int help,     \
+                                cudaStream_t st);                            \
   size_t stage_smem_##SUFFIX(int visc, int tile);                          \
   size_t stage_batch_smem_##SUFFIX(int visc, int tile);
 SWC_DECL_STAGE(f32_s0)

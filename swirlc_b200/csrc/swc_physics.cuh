@@ -519,6 +519,53 @@ __device__ __forceinline__ void riemann(const Prim<T>& l, const Prim<T>& r,
   }
 }
 
+// Fluxes of `ns` transported scalars phi_k with face values phl/phr: the
+// generic branches of the physical flux (m*phi,
+// compressible_navier_stokes.py:419-427), of HLL (hll.py:159-170) and of the
+// HLLC star flux (hllc.py:182-192; wave speeds from the p_dyn-updated states,
+// hllc.py:105-120).
+template <int RIEMANN, typename T, int D>
+__device__ __forceinline__ void scalar_fluxes(const Prim<T>& l,
+                                              const Prim<T>& r, T pdl, T pdr,
+                                              T pe, int ns, const T* phl,
+                                              const T* phr, T* out) {
+  const T ml = l.r * l.u[D], mr = r.r * r.u[D];
+  if constexpr (RIEMANN == 0) {
+    T s_l, s_r;
+    hll_speeds<T, D>(l, r, pe, s_l, s_r);
+    T ds = s_r - s_l;
+    T t1 = dnn(min_(s_r, T(0)) - min_(s_l, T(0)), ds);
+    T t2 = T(1) - t1;
+    T t3 = dnn(s_r * abs_(s_l) - s_l * abs_(s_r), T(2) * ds);
+#pragma unroll
+    for (int k = 0; k < ns; ++k)
+      out[k] = t1 * (mr * phr[k]) + t2 * (ml * phl[k]) -
+               t3 * (mul_rn(r.r, phr[k]) - mul_rn(l.r, phl[k]));
+  } else {
+    Prim<T> lu = l, ru = r;
+    lu.p = pdl;
+    ru.p = pdr;
+    T s_l, s_r;
+    hll_speeds<T, D>(lu, ru, pe, s_l, s_r);
+    T s_m = hllc_contact<T, D>(lu, ru, s_l, s_r);
+    bool c1 = s_l >= T(0);
+    bool c2 = (s_l <= T(0)) && (s_m >= T(0));
+    bool c3 = (s_m <= T(0)) && (s_r >= T(0));
+    bool left = c1 || c2;
+    bool star = !c1 && (c2 || c3);
+    const Prim<T>& q = left ? l : r;
+    T s_k = left ? s_l : s_r;
+    T m = left ? ml : mr;
+#pragma unroll
+    for (int k = 0; k < ns; ++k) {
+      T ph = left ? phl[k] : phr[k];
+      T fk = m * ph;
+      if (star) fk = fk + q.r * (s_m - q.u[D]) * ph * dnn(s_k, s_k - s_m);
+      out[k] = fk;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Viscous flux on the face between cells a (i-1) and b (i) along D
 // (compressible_navier_stokes.py:618-707; diffusion.py:33-109;

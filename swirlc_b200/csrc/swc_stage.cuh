@@ -28,9 +28,9 @@ struct StageArgs {
   int nx, ny, nz, halo;
   long long sx, sz;
   double dx, dy, dz;
-  const void* uk[5];
-  const void* u0[5];
-  void* uout[5];
+  const void* uk[SWC_MAX_FIELDS];
+  const void* u0[SWC_MAX_FIELDS];
+  void* uout[SWC_MAX_FIELDS];
   int mode;
   double c0, c1;
   const double* dt;
@@ -77,19 +77,25 @@ struct Geom {
   static constexpr int NEED = cmax(HR, cmax(ZLO + 1, ZHI));
 };
 
-template <typename T, int SCHEME, bool VISC, int TY, int TX>
+// Shared-memory layout. NS transported scalars and (HELP) the p_dyn helper
+// add reconstructed variables to the 7 primitives rho, u, v, w, e, p, h.
+template <typename T, int SCHEME, bool VISC, int TY, int TX, int NS = 0,
+          bool HELP = false>
 struct Layout {
   using G = Geom<SCHEME, VISC>;
+  static constexpr int NV = 7 + NS + (HELP ? 1 : 0);   // ring variables
+  static constexpr int NCS = 5 + NS + (HELP ? 1 : 0);  // staged fields
+  static constexpr int NF = 5 + NS;                     // flux components
   static constexpr int PW = TY + 2 * G::HR;
   static constexpr int PH = TX + 2 * G::HR;
   static constexpr int PS = PW * PH;
   static constexpr int NT = TX * TY;
   static constexpr int PER = (PS + NT - 1) / NT;  // plane cells per thread
-  static constexpr int RING_ELEMS = G::RING * 7 * PS;
-  static constexpr int STAGE_ELEMS = 5 * PS;
-  static constexpr int FY_ELEMS = 5 * TX * (TY + 1);
-  static constexpr int FX_ELEMS = 5 * (TX + 1) * TY;
-  static constexpr int FZ_ELEMS = 5 * TX * TY;
+  static constexpr int RING_ELEMS = G::RING * NV * PS;
+  static constexpr int STAGE_ELEMS = NCS * PS;
+  static constexpr int FY_ELEMS = NF * TX * (TY + 1);
+  static constexpr int FX_ELEMS = NF * (TX + 1) * TY;
+  static constexpr int FZ_ELEMS = NF * TX * TY;
   static constexpr size_t SMEM =
       sizeof(T) * (size_t)(RING_ELEMS + STAGE_ELEMS + FY_ELEMS + FX_ELEMS +
                            FZ_ELEMS);
@@ -116,21 +122,26 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 // One CTA's work: the TY x TX column at (y0, x0), z segment zb of `a`.
-template <typename T, int SCHEME, int RIEMANN, bool VISC, int TY, int TX>
-__device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
+// NS scalars, HELP (p_ref/rho_ref) and EXT (face and flux overrides from
+// `ext` on the grid's boundary faces) are compiled in only where asked for.
+template <typename T, int SCHEME, int RIEMANN, bool VISC, int TY, int TX,
+          int NS = 0, bool HELP = false, bool EXT = false>
+__device__ __forceinline__ void stage_body(const StageArgs& a,
+                                           const SwcStageExt* ext, const int y0,
                                            const int x0, const int zb) {
   using G = Geom<SCHEME, VISC>;
-  using L = Layout<T, SCHEME, VISC, TY, TX>;
+  using L = Layout<T, SCHEME, VISC, TY, TX, NS, HELP>;
+  constexpr int NV = L::NV, NCS = L::NCS, NF = L::NF;
   constexpr int LO = G::LO, NW = G::NW, HR = G::HR, ZLO = G::ZLO,
                 ZHI = G::ZHI, RING = G::RING;
   constexpr int PW = L::PW, PH = L::PH, PS = L::PS, NT = L::NT, PER = L::PER;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* ring = reinterpret_cast<T*>(smem_raw);
-  T* stg = ring + L::RING_ELEMS;  // [5][PS] conserved plane in flight
-  T* fy = stg + L::STAGE_ELEMS;   // [5][TX][TY+1]
-  T* fx = fy + L::FY_ELEMS;       // [5][TX+1][TY]
-  T* fz = fx + L::FX_ELEMS;       // [5][TX][TY]
+  T* stg = ring + L::RING_ELEMS;  // [NCS][PS] conserved plane in flight
+  T* fy = stg + L::STAGE_ELEMS;   // [NF][TX][TY+1]
+  T* fx = fy + L::FY_ELEMS;       // [NF][TX+1][TY]
+  T* fz = fx + L::FX_ELEMS;       // [NF][TX][TY]
 
   const int tid = threadIdx.x;
   // Cell of this thread. For TY = 16 a warp covers rows w and w + TX/2, whose
@@ -151,9 +162,10 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
   const int nxa = a.nx + 2 * h, nya = a.ny + 2 * h;
   const long long sx = a.sx, sz = a.sz;
 
-  const T* __restrict__ ukp[5];
+  const T* __restrict__ ukp[NCS];
 #pragma unroll
-  for (int v = 0; v < 5; ++v) ukp[v] = static_cast<const T*>(a.uk[v]);
+  for (int v = 0; v < 5 + NS; ++v) ukp[v] = static_cast<const T*>(a.uk[v]);
+  if constexpr (HELP) ukp[5 + NS] = static_cast<const T*>(ext->p_ref);
   const T* __restrict__ pex = static_cast<const T*>(a.pe[0]);
   const T* __restrict__ pey = static_cast<const T*>(a.pe[1]);
   const T* __restrict__ pez = static_cast<const T*>(a.pe[2]);
@@ -170,7 +182,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
     return (-ax - ay) - az;
   };
   auto R = [&](int slot, int v, int px, int py) -> T& {
-    return ring[((slot * 7 + v) * PH + px) * PW + py];
+    return ring[((slot * NV + v) * PH + px) * PW + py];
   };
   // Plane cells this thread stages and converts: idx = tid + k*NT.
   auto cell_valid = [&](int idx, int& xa, int& ya) -> bool {
@@ -188,7 +200,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
       if (cell_valid(idx, xa, ya)) {
         const long long o = zo + xa * sx + ya;
 #pragma unroll
-        for (int v = 0; v < 5; ++v) cp_async(stg + v * PS + idx, ukp[v] + o);
+        for (int v = 0; v < NCS; ++v) cp_async(stg + v * PS + idx, ukp[v] + o);
       }
     }
     cp_async_commit();
@@ -217,6 +229,27 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
       R(slot, 4, px, py) = e;
       R(slot, 5, px, py) = p;
       R(slot, 6, px, py) = hh;
+      if constexpr (NS > 0 || HELP) {
+        const bool ok = cell_valid(idx, xa, ya);
+        const T inv = T(1) / c[0];
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+          R(slot, 7 + k, px, py) = ok ? inv * stg[(5 + k) * PS + idx] : T(0);
+        if constexpr (HELP) {
+          // p_dyn = p - p_ref, zero in the halo layers beyond the grid's
+          // boundary (exchange_halos with DIRICHLET 0 on all sides).
+          const int za = z + h;
+          const bool out =
+              (xa < h && ext->boundary[0][0]) ||
+              (xa >= a.nx + h && ext->boundary[0][1]) ||
+              (ya < h && ext->boundary[1][0]) ||
+              (ya >= a.ny + h && ext->boundary[1][1]) ||
+              (za < h && ext->boundary[2][0]) ||
+              (za >= a.nz + h && ext->boundary[2][1]);
+          R(slot, 7 + NS, px, py) =
+              (ok && !out) ? p - stg[(5 + NS) * PS + idx] : T(0);
+        }
+      }
     }
   };
   const int zfirst = z0 - ZLO - 1;
@@ -229,8 +262,11 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
   //   ta/tb    ring offsets of the t1-/t1+/t2-/t2+ neighbours of the cells
   //            a = i-1 and b = i (viscous cross derivatives)
   auto hsel = [&](int d) -> T { return d == 0 ? dx : (d == 1 ? dy : dz); };
+  //   bside    EXT only: -1, or the side (0 low, 1 high) of the grid boundary
+  //            this face lies on; pidx its index in a face plane [A][B]
+  constexpr int NSA = NS > 0 ? NS : 1;
   auto face = [&](int dn, const int* off, const int* ta, const int* tb, T pe,
-                  T* f) {
+                  int bside, long long pidx, T* f) {
     const int t1 = dn == 0 ? 1 : 0, t2 = dn == 2 ? 1 : 2;
     const int vel[3] = {1 + dn, 1 + t1, 1 + t2};
     Prim<T> ql, qr;
@@ -247,8 +283,131 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
       set_var(ql, v, ng);
       set_var(qr, v, ps);
     }
+    T phl[NSA], phr[NSA];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      const T* base = ring + (7 + q) * PS;
+      T s[NW];
+#pragma unroll
+      for (int k = 0; k < NW; ++k) s[k] = base[off[k]];
+      reconstruct<SCHEME>(s, a.limiter, phl[q], phr[q]);
+    }
+    T pdl = ql.p, pdr = qr.p;
+    if constexpr (HELP) {
+      const T* base = ring + (7 + NS) * PS;
+      T s[NW];
+#pragma unroll
+      for (int k = 0; k < NW; ++k) s[k] = base[off[k]];
+      reconstruct<SCHEME>(s, a.limiter, pdl, pdr);
+    }
+    auto plane_val = [&](const SwcOverride& o) -> T {
+      return o.plane ? static_cast<const T*>(o.plane)[pidx] : T(o.value);
+    };
+    if constexpr (EXT) {
+      // Face BCs on both face states (boundary.py:247-337): a primitive is
+      // set directly, a conservative one divided by the face density.
+      if (bside >= 0) {
+        const int n = ext->nface[dn][bside];
+        for (int i = 0; i < n; ++i) {
+          const SwcOverride& o = ext->face[dn][bside][i];
+          const T val = plane_val(o);
+          const bool cons = o.mode == SWC_FACE_CONSERVATIVE;
+          const T vl = cons ? dnn(val, ql.r) : val;
+          const T vr = cons ? dnn(val, qr.r) : val;
+          const int c = o.var - 1;
+          const int rr = c == dn ? 0 : (c == t1 ? 1 : 2);
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+            if (o.var >= 1 && o.var <= 3 && r == rr) {
+              ql.u[r] = vl;
+              qr.u[r] = vr;
+            }
+          if (o.var == 4) {
+            ql.e = vl;
+            qr.e = vr;
+          }
+#pragma unroll
+          for (int q = 0; q < NS; ++q)
+            if (o.var == 5 + q) {
+              phl[q] = vl;
+              phr[q] = vr;
+            }
+        }
+      }
+    }
     T g[5];
-    riemann<RIEMANN, T, 0>(ql, qr, pe, g);
+    if constexpr (HELP) {
+      if constexpr (RIEMANN == 0) hll_flux<T, 0>(ql, qr, pdl, pdr, pe, g);
+      else hllc_flux<T, 0>(ql, qr, pdl, pdr, pe, g);
+    } else {
+      riemann<RIEMANN, T, 0>(ql, qr, pe, g);
+    }
+    T gs[NSA];
+    if constexpr (NS > 0)
+      scalar_fluxes<RIEMANN, T, 0>(ql, qr, pdl, pdr, pe, NS, phl, phr, gs);
+    // Back to (x, y, z) momentum order.
+    auto rot = [&](const T* gg, T* out) {
+      out[0] = gg[0];
+      out[1] = dn == 0 ? gg[1] : gg[2];
+      out[2] = dn == 1 ? gg[1] : (dn == 0 ? gg[2] : gg[3]);
+      out[3] = dn == 2 ? gg[1] : gg[3];
+      out[4] = gg[4];
+    };
+    // Flux BCs of one type (boundary.py:89-183) on fb (x, y, z order) and
+    // the scalar fluxes fbs.
+    auto flux_bc = [&](int type, T* fb, T* fbs) {
+      if (bside < 0) return;
+      const int n = ext->nflux[dn][bside];
+      for (int i = 0; i < n; ++i) {
+        const SwcOverride& o = ext->flux[dn][bside][i];
+        if (o.mode != type) continue;
+        const T val = plane_val(o);
+#pragma unroll
+        for (int v = 0; v < 5; ++v)
+          if (o.var == v) fb[v] = val;
+#pragma unroll
+        for (int q = 0; q < NS; ++q)
+          if (o.var == 5 + q) fbs[q] = val;
+      }
+    };
+    if constexpr (EXT) {
+      T fc[5];
+      rot(g, fc);
+      flux_bc(SWC_FLUX_CONVECTIVE, fc, gs);
+      T fv[5] = {T(0), T(0), T(0), T(0), T(0)};
+      T fvs[NSA];
+#pragma unroll
+      for (int q = 0; q < NSA; ++q) fvs[q] = T(0);
+      if constexpr (VISC) {
+        T gv[5] = {T(0), T(0), T(0), T(0), T(0)};
+        const int oa = off[LO - 1], ob = off[LO];
+        T ua[3], ub[3], ga[3][3], gb[3][3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          ua[c] = ring[vel[c] * PS + oa];
+          ub[c] = ring[vel[c] * PS + ob];
+        }
+        const T i2t1 = T(2) * hsel(t1), i2t2 = T(2) * hsel(t2);
+        ga[1][1] = (ring[vel[1] * PS + ta[1]] - ring[vel[1] * PS + ta[0]]) / i2t1;
+        gb[1][1] = (ring[vel[1] * PS + tb[1]] - ring[vel[1] * PS + tb[0]]) / i2t1;
+        ga[1][0] = (ring[vel[0] * PS + ta[1]] - ring[vel[0] * PS + ta[0]]) / i2t1;
+        gb[1][0] = (ring[vel[0] * PS + tb[1]] - ring[vel[0] * PS + tb[0]]) / i2t1;
+        ga[2][2] = (ring[vel[2] * PS + ta[3]] - ring[vel[2] * PS + ta[2]]) / i2t2;
+        gb[2][2] = (ring[vel[2] * PS + tb[3]] - ring[vel[2] * PS + tb[2]]) / i2t2;
+        ga[2][0] = (ring[vel[0] * PS + ta[3]] - ring[vel[0] * PS + ta[2]]) / i2t2;
+        gb[2][0] = (ring[vel[0] * PS + tb[3]] - ring[vel[0] * PS + tb[2]]) / i2t2;
+        viscous_flux<T, 0>(ring[oa], ring[ob], ua, ub, ring[5 * PS + oa],
+                           ring[5 * PS + ob], ga, gb, hsel(dn), nu, inv_pr, gv);
+        rot(gv, fv);
+        flux_bc(SWC_FLUX_DIFFUSIVE, fv, fvs);
+      }
+#pragma unroll
+      for (int v = 0; v < 5; ++v) f[v] = fc[v] + fv[v];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) f[5 + q] = gs[q] + fvs[q];
+      flux_bc(SWC_FLUX_TOTAL, f, f + 5);
+      return;
+    }
     if constexpr (VISC) {
       const int oa = off[LO - 1], ob = off[LO];
       T ua[3], ub[3], ga[3][3], gb[3][3];
@@ -271,21 +430,32 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
       viscous_flux<T, 0>(ring[oa], ring[ob], ua, ub, ring[5 * PS + oa],
                          ring[5 * PS + ob], ga, gb, hsel(dn), nu, inv_pr, g);
     }
-    // Back to (x, y, z) momentum order.
-    f[0] = g[0];
-    f[1] = dn == 0 ? g[1] : g[2];
-    f[2] = dn == 1 ? g[1] : (dn == 0 ? g[2] : g[3]);
-    f[3] = dn == 2 ? g[1] : g[3];
-    f[4] = g[4];
+    rot(g, f);
+#pragma unroll
+    for (int q = 0; q < NS; ++q) f[5 + q] = gs[q];
   };
 
-  const int SL = 7 * PS;  // ring slot stride
+  const int SL = NV * PS;  // ring slot stride
   // Face of kind `kind` (0 = x-face at row fxx, 1 = y-face at column fyy,
   // 2 = z-face above plane zc) into the flux buffers.
   auto do_face = [&](int kind, int zc, int fxx, int fyy) {
     int off[NW], ta[4], tb[4];
     T pe;
-    T f[5];
+    T f[NF];
+    // Grid-boundary side and face-plane index of this face (EXT only). The
+    // face stored at i (interior numbering) is face i-1/2: i = 0 is the low
+    // boundary, i = n the high one (boundary.py:140-183).
+    int bside = -1;
+    long long pidx = 0;
+    if constexpr (EXT) {
+      const int i = kind == 0 ? x0 + fxx : (kind == 1 ? y0 + fyy : zc + 1);
+      const int n = kind == 0 ? a.nx : (kind == 1 ? a.ny : a.nz);
+      if (i == 0 && ext->boundary[kind][0]) bside = 0;
+      if (i == n && ext->boundary[kind][1]) bside = 1;
+      if (kind == 0) pidx = (long long)(zc + h) * nya + (y0 + fyy + h);
+      else if (kind == 1) pidx = (long long)(zc + h) * nxa + (x0 + fxx + h);
+      else pidx = (long long)(x0 + fxx + h) * nya + (y0 + fyy + h);
+    }
     if (kind == 2) {
       const int pos = (HR + fxx) * PW + HR + fyy;
 #pragma unroll
@@ -294,9 +464,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
       ta[0] = oa - PW; ta[1] = oa + PW; ta[2] = oa - 1; ta[3] = oa + 1;
       tb[0] = ob - PW; tb[1] = ob + PW; tb[2] = ob - 1; tb[3] = ob + 1;
       pe = pe_at(x0 + fxx + h, y0 + fyy + h, zc + 1 + h);
-      face(2, off, ta, tb, pe, f);
+      face(2, off, ta, tb, pe, bside, pidx, f);
 #pragma unroll
-      for (int v = 0; v < 5; ++v) fz[(v * TX + fxx) * TY + fyy] = f[v];
+      for (int v = 0; v < NF; ++v) fz[(v * TX + fxx) * TY + fyy] = f[v];
     } else {
       const int cs = slot_of(zc) * SL;
       const int dm = (slot_of(zc - 1) - slot_of(zc)) * SL;
@@ -310,13 +480,13 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
       ta[0] = oa - s1; ta[1] = oa + s1; ta[2] = oa + dm; ta[3] = oa + dp;
       tb[0] = ob - s1; tb[1] = ob + s1; tb[2] = ob + dm; tb[3] = ob + dp;
       pe = pe_at(x0 + fxx + h, y0 + fyy + h, zc + h);
-      face(kind, off, ta, tb, pe, f);
+      face(kind, off, ta, tb, pe, bside, pidx, f);
       if (kind == 0) {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) fx[(v * (TX + 1) + fxx) * TY + fyy] = f[v];
+        for (int v = 0; v < NF; ++v) fx[(v * (TX + 1) + fxx) * TY + fyy] = f[v];
       } else {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) fy[(v * TX + fxx) * (TY + 1) + fyy] = f[v];
+        for (int v = 0; v < NF; ++v) fy[(v * TX + fxx) * (TY + 1) + fyy] = f[v];
       }
     }
   };
@@ -332,7 +502,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
   }
   issue_plane(z0 + ZHI - 1);  // plane of the loop's first pass, in flight
   const bool own = (x0 + tx < a.nx) && (y0 + ty < a.ny);
-  T flo[5];
+  T flo[NF];
 
   double dtmin_local = 1e300;
   const double dt_d = a.dt ? *a.dt : 0.0;
@@ -390,7 +560,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
     if (pre) {
       if (own) {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) flo[v] = fz[(v * TX + tx) * TY + ty];
+        for (int v = 0; v < NF; ++v) flo[v] = fz[(v * TX + tx) * TY + ty];
       }
       continue;
     }
@@ -399,9 +569,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
     if (own) {
       const int za = zc + h;
       const long long o = za * sz + (long long)xa_c * sx + ya_c;
-      T ukc[5], u0c[5];
+      T ukc[NF], u0c[NF];
 #pragma unroll
-      for (int v = 0; v < 5; ++v) {
+      for (int v = 0; v < NF; ++v) {
         ukc[v] = __ldg(ukp[v] + o);
         u0c[v] = (a.mode >= SWC_OUT_CONVEX)
                      ? __ldg(static_cast<const T*>(a.u0[v]) + o)
@@ -409,17 +579,20 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
       }
       T src[5] = {T(0), T(0), T(0), T(0), T(0)};
       if (a.gravity_mask) {
-        const T rho_c = R(slot_of(zc), 0, HR + tx, HR + ty);
+        // Buoyancy acts on rho, or on rho - rho_ref with helper states.
+        T rho_c = R(slot_of(zc), 0, HR + tx, HR + ty);
+        if constexpr (HELP)
+          rho_c = rho_c - __ldg(static_cast<const T*>(ext->rho_ref) + o);
 #pragma unroll
         for (int d = 0; d < 3; ++d)
           if (a.gravity_mask & (1 << d))
             src[1 + d] = rho_c * K<T>::grav() * T(a.g[d]);
       }
-      T out[5];
+      T out[NF];
 #pragma unroll
-      for (int v = 0; v < 5; ++v) {
+      for (int v = 0; v < NF; ++v) {
         const T fhi = fz[(v * TX + tx) * TY + ty];
-        T rhs = src[v];
+        T rhs = v < 5 ? src[v] : T(0);
         rhs = rhs - (fx[(v * (TX + 1) + tx + 1) * TY + ty] -
                      fx[(v * (TX + 1) + tx) * TY + ty]) / dx;
         rhs = rhs - (fy[(v * TX + tx) * (TY + 1) + ty + 1] -
@@ -439,7 +612,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
         out[v] = r;
       }
 #pragma unroll
-      for (int v = 0; v < 5; ++v) static_cast<T*>(a.uout[v])[o] = out[v];
+      for (int v = 0; v < NF; ++v) static_cast<T*>(a.uout[v])[o] = out[v];
       if (a.dtmin_out) {
         T u, v, w, e, p, hh;
         cons_to_prim(out[0], out[1], out[2], out[3], out[4],
@@ -475,8 +648,18 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const int y0,
 template <typename T, int SCHEME, int RIEMANN, bool VISC, int TY, int TX>
 __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
     stage_kernel(const StageArgs a) {
-  stage_body<T, SCHEME, RIEMANN, VISC, TY, TX>(a, blockIdx.x * TY,
+  stage_body<T, SCHEME, RIEMANN, VISC, TY, TX>(a, nullptr, blockIdx.x * TY,
                                                blockIdx.y * TX, blockIdx.z);
+}
+
+// Extended stage: NS transported scalars, HELP reference states, face and
+// flux overrides on the grid boundary (one CTA per SM: the ring is larger).
+template <typename T, int SCHEME, int RIEMANN, bool VISC, int TY, int TX,
+          int NS, bool HELP>
+__global__ void __launch_bounds__(TY* TX, 1)
+    stage_kernel_ext(const StageArgs a, const SwcStageExt e) {
+  stage_body<T, SCHEME, RIEMANN, VISC, TY, TX, NS, HELP, true>(
+      a, &e, blockIdx.x * TY, blockIdx.y * TX, blockIdx.z);
 }
 
 // Batched stage: the CTAs of up to SWC_BATCH_CHUNK independent grids in one
@@ -514,8 +697,8 @@ __global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
   const int local = t - b.pre[lo];
   const int nby = (sa.ny + TY - 1) / TY, nbx = (sa.nx + TX - 1) / TX;
   const int by = local % nby, rest = local / nby;
-  stage_body<T, SCHEME, RIEMANN, VISC, TY, TX>(sa, by * TY, (rest % nbx) * TX,
-                                               rest / nbx);
+  stage_body<T, SCHEME, RIEMANN, VISC, TY, TX>(sa, nullptr, by * TY,
+                                               (rest % nbx) * TX, rest / nbx);
 }
 
 }  // namespace swc

@@ -81,6 +81,44 @@ int launch_batch_rm(const StageBatch& b, int nblocks, int tile,
   return launch_batch_tile<T, RM, V, 16, 16>(b, nblocks, st);
 }
 
+// Extended stage (scalars, helper states, face/flux overrides): 16x16 tiles
+// in f32, 8x16 in f64 so that the larger ring fits in shared memory.
+template <typename T, int RM, bool V, int NS, bool HELP>
+int launch_ext_v(const StageArgs& a, const SwcStageExt& e, cudaStream_t st) {
+  constexpr int TY = sizeof(T) == 4 ? 16 : 8, TX = 16;
+  using Lay = Layout<T, SWC_SCHEME, V, TY, TX, NS, HELP>;
+  auto kern = stage_kernel_ext<T, SWC_SCHEME, RM, V, TY, TX, NS, HELP>;
+  static int attr_set = 0;
+  cudaError_t err;
+  if (!attr_set) {
+    err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)Lay::SMEM);
+    if (err != cudaSuccess) return SWC_ERR_LAUNCH;
+    attr_set = 1;
+  }
+  dim3 grid((a.ny + TY - 1) / TY, (a.nx + TX - 1) / TX,
+            (a.nz + a.zseg - 1) / a.zseg);
+  kern<<<grid, TY * TX, Lay::SMEM, st>>>(a, e);
+  note_launch();
+  err = cudaGetLastError();
+  return err == cudaSuccess ? SWC_OK : SWC_ERR_LAUNCH;
+}
+
+template <typename T, int RM, bool V>
+int launch_ext_rm(const StageArgs& a, const SwcStageExt& e, int ns, bool help,
+                  cudaStream_t st) {
+  switch (ns * 2 + (help ? 1 : 0)) {
+    case 0: return launch_ext_v<T, RM, V, 0, false>(a, e, st);
+    case 1: return launch_ext_v<T, RM, V, 0, true>(a, e, st);
+    case 2: return launch_ext_v<T, RM, V, 1, false>(a, e, st);
+    case 3: return launch_ext_v<T, RM, V, 1, true>(a, e, st);
+    case 4: return launch_ext_v<T, RM, V, 2, false>(a, e, st);
+    case 5: return launch_ext_v<T, RM, V, 2, true>(a, e, st);
+    case 6: return launch_ext_v<T, RM, V, 3, false>(a, e, st);
+    default: return launch_ext_v<T, RM, V, 3, true>(a, e, st);
+  }
+}
+
 template <typename T, bool V>
 size_t smem_tile(int tile) {
 #if SWC_MULTI_TILE
@@ -116,6 +154,19 @@ int SWC_CAT(launch_stage_batch_, SWC_SUFFIX)(const StageBatch& b, int nblocks,
                 : launch_batch_rm<T, 0, false>(b, nblocks, tile, st);
   return visc ? launch_batch_rm<T, 1, true>(b, nblocks, tile, st)
               : launch_batch_rm<T, 1, false>(b, nblocks, tile, st);
+}
+
+int SWC_CAT(launch_stage_ext_, SWC_SUFFIX)(const StageArgs& a,
+                                           const SwcStageExt& e, int riemann,
+                                           int visc, int ns, int help,
+                                           cudaStream_t st) {
+  using T = SWC_T;
+  const bool hp = help != 0;
+  if (riemann == SWC_HLL)
+    return visc ? launch_ext_rm<T, 0, true>(a, e, ns, hp, st)
+                : launch_ext_rm<T, 0, false>(a, e, ns, hp, st);
+  return visc ? launch_ext_rm<T, 1, true>(a, e, ns, hp, st)
+              : launch_ext_rm<T, 1, false>(a, e, ns, hp, st);
 }
 
 size_t SWC_CAT(stage_batch_smem_, SWC_SUFFIX)(int visc, int tile) {

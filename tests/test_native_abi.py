@@ -53,6 +53,9 @@ def test_argument_errors_need_no_gpu(lib):
     nat.check(lib.swc_rk_step_noalloc(None, None, None, 3, None, None, None))
   with pytest.raises(ValueError):
     nat.check(lib.swc_batch_step(None, 3, 1, None, None))
+  with pytest.raises(ValueError):
+    nat.check(lib.swc_rk_stage_ext(None, None, None, None, None, None, 0, 0.0,
+                                   0.0, None, None, None))
 
 
 def test_noalloc_limit_matches_header():
@@ -75,12 +78,17 @@ int main(void) {
   printf("SwcFieldBC %zu\n", sizeof(SwcFieldBC));
   printf("SwcClock %zu\n", sizeof(SwcClock));
   printf("SwcBatchMember %zu\n", sizeof(SwcBatchMember));
+  printf("SwcOverride %zu\n", sizeof(SwcOverride));
+  printf("SwcStageExt %zu\n", sizeof(SwcStageExt));
   F(SwcGrid, sx) F(SwcGrid, dz) F(SwcScheme, nu) F(SwcScheme, g)
   F(SwcScheme, pe_axis) F(SwcScheme, zseg) F(SwcBC, value) F(SwcBC, planes)
   F(SwcFieldBC, side) F(SwcClock, step)
   F(SwcBatchMember, u) F(SwcBatchMember, work) F(SwcBatchMember, pe_axis)
   F(SwcBatchMember, bcs) F(SwcBatchMember, clock) F(SwcBatchMember, tile)
   F(SwcBatchMember, zseg)
+  F(SwcOverride, value) F(SwcOverride, plane) F(SwcStageExt, boundary)
+  F(SwcStageExt, nface) F(SwcStageExt, nflux) F(SwcStageExt, face)
+  F(SwcStageExt, flux)
   return 0;
 }
 '''
@@ -103,6 +111,8 @@ def test_struct_layouts_match_header():
   assert c['SwcFieldBC'] == ctypes.sizeof(nat.SwcFieldBC)
   assert c['SwcClock'] == ctypes.sizeof(nat.SwcClock)
   assert c['SwcBatchMember'] == ctypes.sizeof(nat.SwcBatchMember)
+  assert c['SwcOverride'] == ctypes.sizeof(nat.SwcOverride)
+  assert c['SwcStageExt'] == ctypes.sizeof(nat.SwcStageExt)
   for key, off in c.items():
     if '.' not in key:
       continue
