@@ -634,6 +634,74 @@ def update_conservative_cell_averages(cons, cfg):
 # ----------------------------------------------------------------------------
 # RHS (compressible_navier_stokes.py:68-268)
 # ----------------------------------------------------------------------------
+def _interface_bc(bc_by_var, dim, side):
+  """boundary.py:186-236 (_get_bc_dict_along_dim): DIRICHLET or None."""
+  out = {}
+  for name, spec in bc_by_var.items():
+    kind, val = spec[dim][side]
+    if kind is None:
+      continue
+    if bc_kind(kind) != DIRICHLET:
+      raise AssertionError(f'Unsupported interface (face or flux) BC type {kind}.')
+    out[name] = val
+  return out
+
+
+def _plane_value(val, like):
+  if np.isscalar(val) or np.ndim(val) == 0:
+    return like.dtype.type(val)
+  return np.asarray(val, dtype=like.dtype)
+
+
+def update_faces(c_neg, c_pos, p_neg, p_pos, cfg):
+  """boundary.py:340-461 with _face_boundary_update_1d (:239-337), one
+  replica: face values on the planes between halo and interior; as in the
+  reference, the other member of the (conservative, primitive) pair is then
+  recomputed over the whole array. A density face BC is not restated (the
+  reference then drops p and h from the face primitives)."""
+  bcf = (cfgget(cfg, 'bc') or {}).get('cell_faces')
+  if not bcf:
+    return
+  hw = cfg.halo_width
+  for d in DIMS:
+    ax = AXIS[d]
+    for side in (0, 1):
+      bc1 = _interface_bc(bcf, d, side)
+      if not bc1:
+        continue
+      if RHO in bc1:
+        raise NotImplementedError('density face BC')
+      for cons, prim in ((c_neg[d], p_neg[d]), (c_pos[d], p_pos[d])):
+        n = cons[RHO].shape[ax] - 2 * hw
+        idx = hw if side == 0 else hw + n
+        for name, val in bc1.items():
+          if name in cons:
+            pname = conservative_to_primitive_name(name)
+            _set_plane(cons[name], ax, idx, _plane_value(val, cons[name]))
+            prim[pname] = divide_no_nan(cons[name], cons[RHO])
+          else:
+            cname = 'rho_' + name
+            _set_plane(prim[name], ax, idx, _plane_value(val, prim[name]))
+            cons[cname] = cons[RHO] * prim[name]
+
+
+def update_fluxes(flux, cfg, flux_type: str):
+  """boundary.py:89-183, one replica: the flux across the boundary faces
+  (indices hw and hw + n along the dim) set for the given flux type."""
+  bcx = (cfgget(cfg, 'bc') or {}).get('intercell_fluxes')
+  if not bcx or flux_type not in bcx:
+    return flux
+  hw = cfg.halo_width
+  for d in DIMS:
+    ax = AXIS[d]
+    for side in (0, 1):
+      for name, val in _interface_bc(bcx[flux_type], d, side).items():
+        f = flux[d][name]
+        n = f.shape[ax] - 2 * hw
+        _set_plane(f, ax, hw if side == 0 else hw + n, _plane_value(val, f))
+  return flux
+
+
 def rhs(cons: Dict[str, np.ndarray], cfg, helper: Optional[Dict] = None,
         interp_fn=None, apply_bc=True, pe=None) -> Dict[str, np.ndarray]:
   helper = dict(helper or {})
@@ -667,6 +735,7 @@ def rhs(cons: Dict[str, np.ndarray], cfg, helper: Optional[Dict] = None,
            for d in DIMS}
   c_pos = {d: primitive_to_conservative({k: p_pos[d][k] for k in prim_names})
            for d in DIMS}
+  update_faces(c_neg, c_pos, p_neg, p_pos, cfg)
   scheme = cfgget(cfg, 'numeric_flux_scheme')
   if scheme == 'HLL':
     ffn = hll_flux
@@ -676,11 +745,13 @@ def rhs(cons: Dict[str, np.ndarray], cfg, helper: Optional[Dict] = None,
     raise ValueError(f'"{scheme}" is not implemented as a "numeric_flux_scheme".')
   flux = {d: ffn(c_neg[d], c_pos[d], p_neg[d], p_pos[d], h_neg[d], h_pos[d], d,
                  names, pe) for d in DIMS}
+  flux = update_fluxes(flux, cfg, 'convective')
   if cfgget(cfg, 'include_diffusion', False):
-    fd = diffusive_flux(prim, cfg, names)
+    fd = update_fluxes(diffusive_flux(prim, cfg, names), cfg, 'diffusive')
     for d in DIMS:
       for k in names:
         flux[d][k] = flux[d][k] + fd[d][k]
+  flux = update_fluxes(flux, cfg, 'total')
   source = {k: np.zeros_like(v) for k, v in cons.items()}
   src_fns = cfgget(cfg, 'source_functions') or []
   if 'gravity' in src_fns:

@@ -141,14 +141,21 @@ class Solver:
     self.pm = physics_models
     self.dtype = dtype
     self.device = device or torch.device('cuda', torch.cuda.current_device())
-    self.names = list(names or cfg.conservative_variable_names)
-    if self.names[:5] != list(types.BASE_CONSERVATIVE) or len(self.names) != 5:
-      extra = [n for n in self.names if n not in types.BASE_CONSERVATIVE]
-      if extra:
-        raise NotImplementedError(
-            f'Transported scalars {extra} are not supported by the fused '
-            'CUDA path yet.')
-      self.names = list(types.BASE_CONSERVATIVE)
+    names = list(names or cfg.conservative_variable_names)
+    extra = [n for n in names if n not in types.BASE_CONSERVATIVE]
+    missing = [n for n in types.BASE_CONSERVATIVE if n not in names]
+    if missing:
+      raise ValueError(f'Missing conservative variables {missing}.')
+    if len(extra) > 3:
+      raise NotImplementedError(
+          f'{len(extra)} transported scalars {extra}; the fused CUDA path '
+          'takes at most 3.')
+    for n in extra:
+      if not types.is_conservative_name(n):
+        raise ValueError(f'Transported scalar "{n}" must be named rho_<name>.')
+    # rho, rho_u, rho_v, rho_w, rho_e, then the scalars rho_phi.
+    self.names = list(types.BASE_CONSERVATIVE) + extra
+    self.ns = len(extra)
     hw = int(cfg.halo_width)
     nza, nxa, nya = (int(s) for s in shape)
     self.shape = (nza, nxa, nya)
@@ -158,10 +165,6 @@ class Solver:
       raise ValueError(f'Field shape {shape} is too small for halo_width {hw}.')
     self.grid = nat.SwcGrid(self.nx, self.ny, self.nz, hw, nya, nya * nxa,
                             float(cfg.dx), float(cfg.dy), float(cfg.dz))
-    if _CELL_FACE in cfg.bc or _CELL_FLUX in cfg.bc:
-      raise NotImplementedError(
-          'Face and flux boundary conditions are not supported by the fused '
-          'CUDA path yet.')
     sc = nat.SwcScheme()
     sc.dtype = nat.dtype_code(dtype)
     sc.interp = (_INTERP[interp_override] if interp_override
@@ -172,7 +175,7 @@ class Solver:
     sc.limiter = _LIMITER[lim]
     sc.riemann = riemann_code(cfg)
     sc.diffusion = 1 if cfg.include_diffusion else 0
-    sc.nscalars = 0
+    sc.nscalars = self.ns
     sc.gravity_mask = physics_models.gravity_mask()
     sc.zseg = int(getattr(cfg, 'zseg', 0) or 0)
     sc.tile = int(getattr(cfg, 'tile', 0) or 0)
@@ -208,6 +211,7 @@ class Solver:
     else:
       self._bc_cells = cfg.bc.get(_CELL_AVG, {})
     self._build_bcs()
+    self._build_ext()
     self._masked = None
     self._exchange = None
     if self._layout is not None:
@@ -235,10 +239,104 @@ class Solver:
                                     self.dtype, self.device, name)
     self.bcs = arr
 
+  # ------------------------------------------------- face and flux BCs
+  def _side_on_boundary(self, d: int, side: int) -> bool:
+    """Whether this replica's side lies on the boundary of the whole grid
+    (the only faces face/flux BCs act on, boundary.py:140-183, 434-461)."""
+    if self.replicas is None or self.replicas.size == 1:
+      return True
+    c = np.argwhere(self.replicas == self.replica_id)[0]
+    return c[d] == 0 if side == 0 else c[d] == self.replicas.shape[d] - 1
+
+  def _override_value(self, o, val, d: int) -> None:
+    if isinstance(val, (int, float, np.floating, np.integer)):
+      o.value = float(val)
+      o.plane = None
+      return
+    t = _plane(val, d, self.shape, self.dtype, self.device)
+    self._planes.append(t)
+    o.plane = t.data_ptr()
+
+  def _build_ext(self) -> None:
+    """SwcStageExt for the scalars and the cfg's face / flux BCs; use_ext
+    tells whether the plain stage suffices."""
+    e = nat.SwcStageExt()
+    for d in range(3):
+      for side in range(2):
+        e.boundary[d][side] = int(self._side_on_boundary(d, side))
+    prim_names = [types.conservative_to_primitive_name(n) if i else n
+                  for i, n in enumerate(self.names)]
+    faces = self.cfg.bc.get(_CELL_FACE) or {}
+    for name, spec in faces.items():
+      for d, dim in enumerate(types.DIMS):
+        for side in range(2):
+          kind, val = (spec.get(dim) or {}).get(side, (None, None))
+          if kind is None:
+            continue
+          if bc_types.bc_value(kind) != bc_types.BoundaryCondition.DIRICHLET.value:
+            raise ValueError(
+                f'Unsupported interface (face or flux) BC type {kind}. Only'
+                ' "DIRICHLET" or `None` is supported.')
+          if name == types.RHO:
+            raise NotImplementedError(
+                'A density face boundary condition is not supported (the '
+                'reference drops p and h from the face primitives after it).')
+          if name in self.names:
+            var, mode = self.names.index(name), nat.SWC_FACE_CONSERVATIVE
+          elif name in prim_names:
+            var, mode = prim_names.index(name), nat.SWC_FACE_PRIMITIVE
+          else:
+            raise ValueError(
+                f'"{name}" is not a valid primitive or conservative variable'
+                ' name for the face boundary condition update.')
+          if not self._side_on_boundary(d, side):
+            continue
+          n = e.nface[d][side]
+          o = e.face[d][side][n]
+          o.var, o.mode = var, mode
+          self._override_value(o, val, d)
+          e.nface[d][side] = n + 1
+    fluxes = self.cfg.bc.get(_CELL_FLUX) or {}
+    codes = {bc_types.BoundaryFluxType.CONVECTIVE.value: nat.SWC_FLUX_CONVECTIVE,
+             bc_types.BoundaryFluxType.DIFFUSIVE.value: nat.SWC_FLUX_DIFFUSIVE,
+             bc_types.BoundaryFluxType.TOTAL.value: nat.SWC_FLUX_TOTAL}
+    for ftype, per_var in fluxes.items():
+      key = getattr(ftype, 'value', ftype)
+      if key not in codes:
+        raise ValueError(f'Unknown flux boundary type {ftype}.')
+      for name, spec in per_var.items():
+        if name not in self.names:
+          raise ValueError(
+              f'{name} cannot be specified by a flux boundary condition. Only'
+              f' conservative variables {self.names} can be specified with a'
+              ' flux boundary condition.')
+        for d, dim in enumerate(types.DIMS):
+          for side in range(2):
+            kind, val = (spec.get(dim) or {}).get(side, (None, None))
+            if kind is None or not self._side_on_boundary(d, side):
+              continue
+            if bc_types.bc_value(kind) != bc_types.BoundaryCondition.DIRICHLET.value:
+              raise ValueError(
+                  f'Unsupported interface (face or flux) BC type {kind}. Only'
+                  ' "DIRICHLET" or `None` is supported.')
+            n = e.nflux[d][side]
+            o = e.flux[d][side][n]
+            o.var, o.mode = self.names.index(name), codes[key]
+            self._override_value(o, val, d)
+            e.nflux[d][side] = n + 1
+    if faces and self.cfg.include_diffusion:
+      raise NotImplementedError(
+          'Face boundary conditions are not supported with diffusion enabled'
+          ' at this time.')
+    has_overrides = any(e.nface[d][s] or e.nflux[d][s]
+                        for d in range(3) for s in range(2))
+    self.ext = e
+    self.use_ext = bool(self.ns or has_overrides)
+
   # -------------------------------------------------------------- kernels
   def check_fields(self, fields: Sequence[torch.Tensor]) -> None:
-    if len(fields) != 5:
-      raise ValueError('Expected 5 conserved fields.')
+    if len(fields) != len(self.names):
+      raise ValueError(f'Expected {len(self.names)} conserved fields.')
     for f in fields:
       if (tuple(f.shape) != self.shape or f.dtype != self.dtype or
           not f.is_cuda or not f.is_contiguous()):
@@ -286,7 +384,22 @@ class Solver:
 
   def stage(self, uk, u0, uout, mode: int, c0: float = 0.0, c1: float = 0.0,
             dt: Optional[torch.Tensor] = None,
-            dtmin_out: Optional[torch.Tensor] = None) -> None:
+            dtmin_out: Optional[torch.Tensor] = None,
+            helper: Optional[Dict[str, torch.Tensor]] = None) -> None:
+    if self.use_ext or helper:
+      e = self.ext
+      if helper:
+        e = nat.SwcStageExt.from_buffer_copy(self.ext)
+        e.p_ref = self._helper_field(helper, 'p_ref').data_ptr()
+        e.rho_ref = self._helper_field(helper, 'rho_ref').data_ptr()
+      nat.check(nat.load().swc_rk_stage_ext(
+          ctypes.byref(self.grid), ctypes.byref(self.scheme), ctypes.byref(e),
+          nat.ptr_array(uk), nat.ptr_array(u0) if u0 is not None else None,
+          nat.ptr_array(uout), mode, float(c0), float(c1),
+          dt.data_ptr() if dt is not None else None,
+          dtmin_out.data_ptr() if dtmin_out is not None else None,
+          nat.stream_ptr()), 'rk stage')
+      return
     nat.check(nat.load().swc_rk_stage(
         ctypes.byref(self.grid), ctypes.byref(self.scheme),
         nat.ptr_array(uk), nat.ptr_array(u0) if u0 is not None else None,
@@ -294,6 +407,14 @@ class Solver:
         dt.data_ptr() if dt is not None else None,
         dtmin_out.data_ptr() if dtmin_out is not None else None,
         nat.stream_ptr()), 'rk stage')
+
+  def _helper_field(self, helper, name) -> torch.Tensor:
+    t = utils.as_tensor3d(helper[name])
+    if (tuple(t.shape) != self.shape or t.dtype != self.dtype or
+        not t.is_cuda or not t.is_contiguous()):
+      raise ValueError(f'Helper variable {name} must be a contiguous CUDA '
+                       f'tensor of shape {self.shape} and dtype {self.dtype}.')
+    return t
 
   def cfl_reduce(self, fields, dtmin_out: torch.Tensor) -> None:
     nat.check(nat.load().swc_cfl_reduce(
@@ -304,41 +425,47 @@ class Solver:
   def new_fields(self, zero: bool = True) -> List[torch.Tensor]:
     alloc = torch.zeros if zero else torch.empty
     return [alloc(self.shape, dtype=self.dtype, device=self.device)
-            for _ in range(5)]
+            for _ in range(len(self.names))]
 
-  def rhs(self, fields: Sequence[torch.Tensor]) -> List[torch.Tensor]:
+  def rhs(self, fields: Sequence[torch.Tensor],
+          helper: Optional[Dict[str, torch.Tensor]] = None) -> List[torch.Tensor]:
     """Functional RHS: copies, fills halos of the copy, returns dU/dt."""
     work = [f.clone() for f in fields]
     self.fill_halos(work)
     out = self.new_fields(zero=True)
-    self.stage(work, None, out, nat.SWC_OUT_RHS)
+    self.stage(work, None, out, nat.SWC_OUT_RHS, helper=helper)
     return out
 
-  def rk3(self, fields: Sequence[torch.Tensor], dt: float) -> List[torch.Tensor]:
+  def rk3(self, fields: Sequence[torch.Tensor], dt: float,
+          helper: Optional[Dict[str, torch.Tensor]] = None) -> List[torch.Tensor]:
     """Functional SSP-RK3 step (rk3.py:87-120) returning new fields."""
     dtt = self.dt_tensor(dt)
     u0 = [f.clone() for f in fields]
     self.fill_halos(u0)
     u1 = self.new_fields(zero=False)
-    self.stage(u0, None, u1, nat.SWC_OUT_EULER, dt=dtt)
+    self.stage(u0, None, u1, nat.SWC_OUT_EULER, dt=dtt, helper=helper)
     self.fill_halos(u1)
     u2 = self.new_fields(zero=False)
-    self.stage(u1, u0, u2, nat.SWC_OUT_CONVEX, 0.75, 0.25, dt=dtt)
+    self.stage(u1, u0, u2, nat.SWC_OUT_CONVEX, 0.75, 0.25, dt=dtt,
+               helper=helper)
     self.fill_halos(u2)
-    self.stage(u2, u0, u1, nat.SWC_OUT_CONVEX, 1.0 / 3.0, 2.0 / 3.0, dt=dtt)
+    self.stage(u2, u0, u1, nat.SWC_OUT_CONVEX, 1.0 / 3.0, 2.0 / 3.0, dt=dtt,
+               helper=helper)
     self.fill_halos(u1)
     return u1
 
-  def rk2(self, fields: Sequence[torch.Tensor], dt: float) -> List[torch.Tensor]:
+  def rk2(self, fields: Sequence[torch.Tensor], dt: float,
+          helper: Optional[Dict[str, torch.Tensor]] = None) -> List[torch.Tensor]:
     """Functional RK2 step (rk2.py:63-86) returning new fields."""
     dtt = self.dt_tensor(dt)
     u0 = [f.clone() for f in fields]
     self.fill_halos(u0)
     u1 = self.new_fields(zero=False)
-    self.stage(u0, None, u1, nat.SWC_OUT_EULER, dt=dtt)
+    self.stage(u0, None, u1, nat.SWC_OUT_EULER, dt=dtt, helper=helper)
     self.fill_halos(u1)
     u2 = self.new_fields(zero=False)
-    self.stage(u1, u0, u2, nat.SWC_OUT_AVERAGE, 0.5, 0.0, dt=dtt)
+    self.stage(u1, u0, u2, nat.SWC_OUT_AVERAGE, 0.5, 0.0, dt=dtt,
+               helper=helper)
     self.fill_halos(u2)
     return u2
 
@@ -354,7 +481,8 @@ class Stepper:
 
   def __init__(self, solver: Solver, fields: Sequence[torch.Tensor],
                dt: float = 0.0, cfl: float = 0.0, t_end: float = 0.0,
-               scheme: str = 'rk3'):
+               scheme: str = 'rk3',
+               helper: Optional[Dict[str, torch.Tensor]] = None):
     solver.check_fields(fields)
     self.s = solver
     self.u = list(fields)
@@ -371,6 +499,7 @@ class Stepper:
     self.clock[3] = float(cfl)
     self.clock[4] = float(t_end)
     self.cfl = float(cfl)
+    self.helper = dict(helper) if helper else None
     if self.cfl > 0.0:
       solver.cfl_reduce(self.u, self.clock[2:3])
     self.graph: Optional[torch.cuda.CUDAGraph] = None
@@ -380,7 +509,30 @@ class Stepper:
     return self.clock[1:2]
 
   def _launch_step(self):
-    """One step through swc_rk_step (halo fills, fused stages, clock)."""
+    """One step through swc_rk_step (halo fills, fused stages, clock); the
+    extended stage (scalars, helper states, face/flux BCs) is composed here
+    from the same pieces."""
+    if self.s.use_ext or self.helper:
+      lib = nat.load()
+      s, u, w1, w2 = self.s, self.u, self.w1, self.w2
+      dt, dtmin = self.clock[1:2], self.clock[2:3]
+      nat.check(lib.swc_clock_begin_step(self.clock.data_ptr(),
+                                         nat.stream_ptr()))
+      s.fill_halos(u)
+      s.stage(u, None, w1, nat.SWC_OUT_EULER, dt=dt, helper=self.helper)
+      s.fill_halos(w1)
+      if self.scheme == 'rk3':
+        s.stage(w1, u, w2, nat.SWC_OUT_CONVEX, 0.75, 0.25, dt=dt,
+                helper=self.helper)
+        s.fill_halos(w2)
+        s.stage(w2, u, u, nat.SWC_OUT_CONVEX, 1.0 / 3.0, 2.0 / 3.0, dt=dt,
+                dtmin_out=dtmin, helper=self.helper)
+      else:
+        s.stage(w1, u, u, nat.SWC_OUT_AVERAGE, 0.5, 0.0, dt=dt,
+                dtmin_out=dtmin, helper=self.helper)
+      nat.check(lib.swc_clock_end_step(self.clock.data_ptr(),
+                                       nat.stream_ptr()))
+      return
     work = self.w1 + self.w2
     nat.check(nat.load().swc_rk_step(
         ctypes.byref(self.s.grid), ctypes.byref(self.s.scheme), self.s.bcs,

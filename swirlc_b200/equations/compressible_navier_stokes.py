@@ -61,22 +61,36 @@ def _check_cfg(cfg):
         ' this time.')
 
 
-def _ordered_fields(conservative) -> list:
+def _ordered_fields(conservative, cfg=None) -> list:
+  """Fields in the solver's order: rho, rho_u, rho_v, rho_w, rho_e, then the
+  transported scalars in the order of cfg.conservative_variable_names."""
   missing = [n for n in types.BASE_CONSERVATIVE if n not in conservative]
   if missing:
     raise ValueError(f'Missing conservative variables {missing}.')
   extra = [n for n in conservative if n not in types.BASE_CONSERVATIVE]
-  if extra:
-    raise NotImplementedError(
-        f'Transported scalars {extra} are not supported by the fused CUDA '
-        'path yet.')
+  if cfg is not None and extra:
+    order = [n for n in cfg.conservative_variable_names if n in extra]
+    if set(order) != set(extra):
+      raise ValueError(
+          f'Transported scalars {extra} are not all in the configuration '
+          f'({cfg.conservative_variable_names}).')
+    extra = order
   out = []
-  for n in types.BASE_CONSERVATIVE:
+  for n in list(types.BASE_CONSERVATIVE) + extra:
     t = utils.as_tensor3d(conservative[n])
     if not t.is_cuda:
       raise ValueError(f'Field {n} must be a CUDA tensor.')
     out.append(t.contiguous())
   return out
+
+
+def helper_states(helper_vars):
+  """The hydrostatic reference states when both are given (the reference
+  uses them only then, compressible_navier_stokes.py:309)."""
+  if helper_vars and 'p_ref' in helper_vars and 'rho_ref' in helper_vars:
+    return {'p_ref': utils.as_tensor3d(helper_vars['p_ref']).contiguous(),
+            'rho_ref': utils.as_tensor3d(helper_vars['rho_ref']).contiguous()}
+  return None
 
 
 def get_rhs_fn(replicas: np.ndarray, cfg, physics_models):
@@ -86,14 +100,10 @@ def get_rhs_fn(replicas: np.ndarray, cfg, physics_models):
                        getattr(cfg, '_interp_override', None))
 
   def rhs(replica_id, conservative: Dict, helper_vars: Dict) -> Dict:
-    if helper_vars and ('p_ref' in helper_vars or 'rho_ref' in helper_vars):
-      raise NotImplementedError(
-          'Helper reference states (p_ref, rho_ref) are not supported by the '
-          'fused CUDA path yet.')
-    fields = _ordered_fields(conservative)
+    fields = _ordered_fields(conservative, cfg)
     solver = cache.get(replica_id, fields)
-    out = solver.rhs(fields)
-    res = dict(zip(types.BASE_CONSERVATIVE, out))
+    out = solver.rhs(fields, helper_states(helper_vars))
+    res = dict(zip(solver.names, out))
     return {k: utils.like_input(res[k], conservative[k]) for k in conservative}
 
   rhs._swc_cache = cache  # lets rk3/rk2 run the fused in-place stages

@@ -12,13 +12,13 @@ def integrate(replica_id, replicas, state_0, helper_vars, cfg, physics_models,
   """rk2.py:30-86."""
   del replicas, physics_models
   cache = getattr(rhs_fn, '_swc_cache', None)
-  if cache is not None and not (helper_vars and 'p_ref' in helper_vars):
+  if cache is not None:
     from swirlc_b200.equations import compressible_navier_stokes as cns
-    from swirlc_b200.common import types, utils
-    fields = cns._ordered_fields(state_0)
+    from swirlc_b200.common import utils
+    fields = cns._ordered_fields(state_0, cfg)
     solver = cache.get(replica_id, fields)
-    out = solver.rk2(fields, cfg.dt)
-    res = dict(zip(types.BASE_CONSERVATIVE, out))
+    out = solver.rk2(fields, cfg.dt, cns.helper_states(helper_vars))
+    res = dict(zip(solver.names, out))
     return {k: utils.like_input(res[k], state_0[k]) for k in state_0}
   dt_t = _stages.dt_tensor(cfg.dt, _stages.first_device(state_0))
   df = rhs_fn(replica_id, state_0, helper_vars)
