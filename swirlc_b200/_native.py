@@ -41,6 +41,7 @@ EXPORTED = (
     'swc_clock_end_step', 'swc_reconstruct', 'swc_riemann_flux',
     'swc_wave_speeds', 'swc_stencil', 'swc_rk_combine', 'swc_rk_step',
     'swc_rk_step_noalloc', 'swc_batch_step', 'swc_rk_stage_ext',
+    'swc_rk_stage_vjp',
 )
 
 # Built-in work space of swc_rk_step_noalloc (SWC_NOALLOC_MAX_BYTES).
@@ -161,6 +162,10 @@ def load(require_cuda: bool = True) -> ctypes.CDLL:
                                        ctypes.POINTER(SwcScheme),
                                        ctypes.POINTER(SwcStageExt), pp, pp, pp,
                                        i32, dbl, dbl, vp, vp, vp]
+      lib.swc_rk_stage_vjp.argtypes = [ctypes.POINTER(SwcGrid),
+                                       ctypes.POINTER(SwcScheme),
+                                       ctypes.POINTER(SwcFieldBC), pp, pp, dbl,
+                                       pp, vp, pp, vp]
       lib.swc_batch_step.argtypes = [ctypes.POINTER(SwcScheme), i32, i32,
                                      ctypes.POINTER(SwcBatchMember), vp]
       lib.swc_rk_step_noalloc.argtypes = [ctypes.POINTER(SwcGrid),

@@ -1,0 +1,195 @@
+"""Gradients of whole runs: the discrete adjoint of the fused RK stages.
+
+The reference differentiates its TensorFlow graph with GradientTape. Here a
+run of SSP-RK3 (rk3.py:87-120) or RK2 (rk2.py:69-86) steps is reversed with
+the stage vector-Jacobian product of the library (`swc_rk_stage_vjp`), with
+checkpointing: the forward run keeps the state every `checkpoint_every`
+steps; the backward sweep recomputes one segment at a time, keeping that
+segment's stage states, and walks back through it. The time steps are those
+of the forward run and are held fixed (not differentiated), as in the
+reference's KH set-up where dt is computed once on the host.
+
+For a step u -> u' with stages
+  u1 = u + dt L(u),  u2 = 3/4 u + 1/4 (u1 + dt L(u1)),
+  u' = 1/3 u + 2/3 (u2 + dt L(u2)),
+the reverse of a cotangent g of u' is
+  g2 = 2/3 g + V(u2, g, 2/3 dt),   g1 = 1/4 g2 + V(u1, g2, 1/4 dt),
+  g_u = 1/3 g + 3/4 g2 + g1 + V(u, g1, dt),
+where V(uk, lam, beta) = beta H^T J_L(H uk)^T lam (the library call). The
+derivative with respect to the kinematic viscosity nu is accumulated by the
+same calls.
+"""
+
+import ctypes
+from typing import List, Optional, Sequence, Tuple
+
+import torch
+
+from swirlc_b200 import _native as nat
+from swirlc_b200 import engine
+
+
+class RunAdjoint:
+  """A forward run with checkpoints and its reverse sweep for one solver.
+
+  Args:
+    solver: an `engine.Solver` (WENO5 + HLLC, optionally viscous).
+    checkpoint_every: steps between stored states.
+    scheme: 'rk3' or 'rk2'.
+  """
+
+  def __init__(self, solver: engine.Solver, checkpoint_every: int = 20,
+               scheme: str = 'rk3'):
+    if scheme not in ('rk3', 'rk2'):
+      raise NotImplementedError(f'"{scheme}" is not implemented as an '
+                                '"time_integration_scheme".')
+    if checkpoint_every < 1:
+      raise ValueError('checkpoint_every must be >= 1.')
+    self.s = solver
+    self.k = int(checkpoint_every)
+    self.order = 3 if scheme == 'rk3' else 2
+    self.checkpoints: List[List[torch.Tensor]] = []
+    self.dts: List[float] = []
+    self._scratch = [torch.empty(solver.shape, dtype=solver.dtype,
+                                 device=solver.device) for _ in range(14)]
+    self._vout = solver.new_fields(zero=True)
+    self._nu_bar = torch.zeros(1, dtype=torch.float64, device=solver.device)
+
+  # ------------------------------------------------------------- forward
+  def _step(self, u, dt, keep: Optional[list] = None):
+    """One step in place on u with fixed dt; `keep` receives the halo-filled
+    stage states (u, u1, u2) when given."""
+    s = self.s
+    dtt = s.dt_tensor(dt)
+    s.fill_halos(u)
+    u0 = [f.clone() for f in u]
+    w1 = s.new_fields(zero=False)
+    s.stage(u0, None, w1, nat.SWC_OUT_EULER, dt=dtt)
+    s.fill_halos(w1)
+    if self.order == 3:
+      w2 = s.new_fields(zero=False)
+      s.stage(w1, u0, w2, nat.SWC_OUT_CONVEX, 0.75, 0.25, dt=dtt)
+      s.fill_halos(w2)
+      s.stage(w2, u0, u, nat.SWC_OUT_CONVEX, 1.0 / 3.0, 2.0 / 3.0, dt=dtt)
+      if keep is not None:
+        keep.append((u0, w1, w2))
+    else:
+      s.stage(w1, u0, u, nat.SWC_OUT_AVERAGE, 0.5, 0.0, dt=dtt)
+      if keep is not None:
+        keep.append((u0, w1))
+
+  def run(self, fields: Sequence[torch.Tensor],
+          dts: Sequence[float]) -> List[torch.Tensor]:
+    """Advances a copy of `fields` by len(dts) steps, keeping checkpoints."""
+    self.s.check_fields(fields)
+    self.dts = [float(d) for d in dts]
+    u = [f.detach().clone() for f in fields]
+    self.checkpoints = []
+    for i, dt in enumerate(self.dts):
+      if i % self.k == 0:
+        self.checkpoints.append([f.clone() for f in u])
+      self._step(u, dt)
+    self.s.fill_halos(u)
+    return u
+
+  # ------------------------------------------------------------ backward
+  def _vjp(self, uk, lam, beta) -> List[torch.Tensor]:
+    s = self.s
+    nat.check(nat.load().swc_rk_stage_vjp(
+        ctypes.byref(s.grid), ctypes.byref(s.scheme), s.bcs,
+        nat.ptr_array(uk), nat.ptr_array(lam), float(beta),
+        nat.ptr_array(self._vout), self._nu_bar.data_ptr(),
+        nat.ptr_array(self._scratch), nat.stream_ptr()), 'stage vjp')
+    return self._vout
+
+  def _interior_only(self, fields):
+    hw = self.s.hw
+    out = []
+    for f in fields:
+      g = torch.zeros_like(f)
+      g[hw:-hw, hw:-hw, hw:-hw] = f[hw:-hw, hw:-hw, hw:-hw]
+      out.append(g)
+    return out
+
+  def backward(self, grad_out: Sequence[torch.Tensor]
+               ) -> Tuple[List[torch.Tensor], float]:
+    """Cotangent of the initial fields and d/dnu for a cotangent of the final
+    fields (interior cells; halos are ignored)."""
+    if not self.checkpoints:
+      raise RuntimeError('backward() needs a run() first.')
+    g = self._interior_only([x.to(self.s.dtype) for x in grad_out])
+    self._nu_bar.zero_()
+    nsteps = len(self.dts)
+    for c in reversed(range(len(self.checkpoints))):
+      first = c * self.k
+      last = min(first + self.k, nsteps)
+      u = [f.clone() for f in self.checkpoints[c]]
+      stages = []
+      for i in range(first, last):
+        self._step(u, self.dts[i], keep=stages)
+      for i in reversed(range(first, last)):
+        dt = self.dts[i]
+        st = stages[i - first]
+        if self.order == 3:
+          u0, u1, u2 = st
+          v = self._vjp(u2, g, 2.0 / 3.0 * dt)
+          g2 = [2.0 / 3.0 * a + b for a, b in zip(g, v)]
+          v = self._vjp(u1, g2, 0.25 * dt)
+          g1 = [0.25 * a + b for a, b in zip(g2, v)]
+          v = self._vjp(u0, g1, dt)
+          g = [a / 3.0 + 0.75 * b + c + d for a, b, c, d in zip(g, g2, g1, v)]
+        else:
+          u0, u1 = st
+          v = self._vjp(u1, g, 0.5 * dt)
+          g1 = [0.5 * a + b for a, b in zip(g, v)]
+          v = self._vjp(u0, g1, dt)
+          g = [0.5 * a + b + c for a, b, c in zip(g, g1, v)]
+        g = self._interior_only(g)
+      del stages
+    return g, float(self._nu_bar.item())
+
+
+class _Run(torch.autograd.Function):
+  """Forward run / reverse sweep as one autograd node."""
+
+  @staticmethod
+  def forward(ctx, runner, dts, nu, *fields):
+    runner.s.scheme.nu = float(nu)
+    out = runner.run(fields, dts)
+    ctx.runner = runner
+    ctx.nu_meta = (nu.dtype, nu.device)
+    return tuple(out)
+
+  @staticmethod
+  def backward(ctx, *grads):
+    grads = [torch.zeros_like(ctx.runner.checkpoints[0][0]) if g is None else g
+             for g in grads]
+    gin, nub = ctx.runner.backward(grads)
+    dtype, device = ctx.nu_meta
+    return (None, None, torch.tensor(nub, dtype=dtype, device=device),
+            *gin)
+
+
+def simulate(runner: RunAdjoint, fields: Sequence[torch.Tensor],
+             dts: Sequence[float], nu: torch.Tensor) -> Tuple[torch.Tensor, ...]:
+  """Differentiable run: the final fields as a function of the initial
+  fields and of the kinematic viscosity `nu` (a 0-d tensor)."""
+  return _Run.apply(runner, list(dts), nu, *fields)
+
+
+def vorticity_energy(fields: Sequence[torch.Tensor], hw: int, dx: float,
+                     dy: float, dz: float) -> torch.Tensor:
+  """Loss of the adjoint benchmark: integral of |omega|^2 / 2 over the
+  periodic interior, omega = curl(u) by central differences, u = rho_u/rho.
+  Axes of the stored fields are (z, x, y)."""
+  sl = (slice(hw, -hw),) * 3
+  rho, ru, rv, rw = (f[sl] for f in fields[:4])
+  u, v, w = ru / rho, rv / rho, rw / rho
+
+  def d(f, axis, h):
+    return (torch.roll(f, -1, axis) - torch.roll(f, 1, axis)) / (2.0 * h)
+
+  wx = d(w, 2, dy) - d(v, 0, dz)
+  wy = d(u, 0, dz) - d(w, 1, dx)
+  wz = d(v, 1, dx) - d(u, 2, dy)
+  return 0.5 * (wx * wx + wy * wy + wz * wz).sum() * (dx * dy * dz)

@@ -1,0 +1,856 @@
+// Reverse mode (vector-Jacobian product) of one fused RK stage for WENO5 +
+// HLLC (+ viscous) on a halo-filled state: the discrete adjoint used to
+// differentiate whole runs (gradients with respect to the initial state and
+// to the kinematic viscosity nu). For a stage out = A*u0 + B*(uk + dt*L(uk))
+// the caller needs lambda_out^T dout/duk = B*lambda + B*dt*H^T J_L^T lambda,
+// where H is the halo fill; swc_rk_stage_vjp computes
+//   vout = beta * H^T J_L(H uk)^T lambda   (beta = B*dt),
+//   nu_bar += beta * lambda . dL/dnu.
+//
+// L(u)_c = S_c - sum_d (F_d[c+1/2] - F_d[c-1/2]) / h_d, so the cotangent of a
+// face flux is Fbar = beta * (lambda_right - lambda_left) / h_d. Each face is
+// recomputed forward (reconstruction, Riemann flux, viscous flux) and then
+// reversed by hand; the reverse of every piece follows the forward code in
+// swc_physics.cuh line by line. Primitive cotangents (rho, u, v, w, e, p, h)
+// are gathered per cell first and turned into conserved cotangents once per
+// cell (the reverse of cons_to_prim), then the halo fill is reversed dim by
+// dim in the order z, y, x.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "swc_launch.h"
+#include "swirlc_b200.h"
+
+namespace swc {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Reverse of the pieces of one face flux.
+// ---------------------------------------------------------------------------
+
+// WENO5 face value from v[0..4] (right face of v[2] when RIGHT, left face of
+// v[2] otherwise): vb[k] += dout/dv[k] * ob.
+template <typename T, bool RIGHT>
+__device__ __forceinline__ void weno5_vjp(const T* v, T ob, T* vb) {
+  constexpr double A[3][5] = {{0, 0, 1, -2, 1}, {0, 1, -2, 1, 0}, {1, -2, 1, 0, 0}};
+  constexpr double Bc[3][5] = {{0, 0, 3, -4, 1}, {0, 1, 0, -1, 0}, {1, -4, 3, 0, 0}};
+  constexpr double QR[3][5] = {{0, 0, 1.0 / 3, 5.0 / 6, -1.0 / 6},
+                               {0, -1.0 / 6, 5.0 / 6, 1.0 / 3, 0},
+                               {1.0 / 3, -7.0 / 6, 11.0 / 6, 0, 0}};
+  constexpr double QL[3][5] = {{0, 0, 11.0 / 6, -7.0 / 6, 1.0 / 3},
+                               {0, 1.0 / 3, 5.0 / 6, -1.0 / 6, 0},
+                               {-1.0 / 6, 5.0 / 6, 1.0 / 3, 0, 0}};
+  constexpr double DR[3] = {0.3, 0.6, 0.1}, DL[3] = {0.1, 0.6, 0.3};
+  const T c1312 = T(13.0 / 12.0), eps = T(1e-6);
+  T av[3], bv[3], be[3], al[3], q[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    T sa = T(0), sb = T(0), sq = T(0);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      sa += T(A[r][k]) * v[k];
+      sb += T(Bc[r][k]) * v[k];
+      sq += T(RIGHT ? QR[r][k] : QL[r][k]) * v[k];
+    }
+    av[r] = sa;
+    bv[r] = sb;
+    q[r] = sq;
+    be[r] = c1312 * sa * sa + T(0.25) * sb * sb + eps;
+    al[r] = T(RIGHT ? DR[r] : DL[r]) / (be[r] * be[r]);
+  }
+  const T S = al[0] + al[1] + al[2];
+  const T out = (al[0] * q[0] + al[1] * q[1] + al[2] * q[2]) / S;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const T qb = ob * al[r] / S;
+    const T ab = ob * (q[r] - out) / S;
+    const T bb = T(-2) * ab * al[r] / be[r];
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+      vb[k] += qb * T(RIGHT ? QR[r][k] : QL[r][k]) +
+               bb * (T(2) * c1312 * av[r] * T(A[r][k]) +
+                     T(0.5) * bv[r] * T(Bc[r][k]));
+  }
+}
+
+// Primitive cotangents of one face state, rotated frame (u[0] normal).
+template <typename T>
+struct PrimBar {
+  T r, u[3], e, p, h;
+  __device__ __forceinline__ void zero() {
+    r = e = p = h = T(0);
+    u[0] = u[1] = u[2] = T(0);
+  }
+};
+
+// d sqrt(x) = dx / (2 sqrt(x)), zero where the root is zero.
+template <typename T>
+__device__ __forceinline__ T dsqrt(T root, T bar) {
+  return root > T(0) ? bar / (T(2) * root) : T(0);
+}
+
+// Reverse of hllc_flux<T, 0> with p_dyn = p (no helper states): fb is the
+// cotangent of the 5 flux components (rotated momentum order).
+template <typename T>
+__device__ __forceinline__ void hllc_vjp(const Prim<T>& l, const Prim<T>& r,
+                                         T pe, const T* fb, PrimBar<T>& lb,
+                                         PrimBar<T>& rb) {
+  const T gam = K<T>::gamma(), gm1 = K<T>::gm1();
+  // ---- forward
+  const T cl = sqrt_(gam * l.p / l.r), cr = sqrt_(gam * r.p / r.r);
+  const T rl = sqrt_(l.r), rr = sqrt_(r.r);
+  const T den = rl + rr;
+  const T inv = den == T(0) ? T(0) : T(1) / den;
+  T nu_[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) nu_[i] = rl * l.u[i] + rr * r.u[i];
+  T ru[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) ru[i] = nu_[i] * inv;
+  const T nh = rl * l.h + rr * r.h;
+  const T rh = nh * inv;
+  const T hs = rh - T(0.5) * (ru[0] * ru[0] + ru[1] * ru[1] + ru[2] * ru[2]) - pe;
+  const T rc = sqrt_(gm1 * hs);
+  const T sla = l.u[0] - cl, slb = ru[0] - rc;
+  const T sra = r.u[0] + cr, srb = ru[0] + rc;
+  const bool lmin_a = sla <= slb, rmax_a = sra >= srb;
+  const T s_l = lmin_a ? sla : slb, s_r = rmax_a ? sra : srb;
+  const T vl = l.u[0], vr = r.u[0];
+  const T num = (r.p - l.p) + l.r * vl * (s_l - vl) - r.r * vr * (s_r - vr);
+  const T dd = l.r * (s_l - vl) - r.r * (s_r - vr);
+  T s_m = dd == T(0) ? T(0) : num / dd;
+  const bool clamp = abs_(s_m) < T(1e-6) || dd == T(0);
+  if (abs_(s_m) < T(1e-6)) s_m = T(0);
+  const bool c1 = s_l >= T(0);
+  const bool c2 = (s_l <= T(0)) && (s_m >= T(0));
+  const bool c3 = (s_m <= T(0)) && (s_r >= T(0));
+  const bool left = c1 || c2;
+  const bool star = !c1 && (c2 || c3);
+  const Prim<T>& q = left ? l : r;
+  PrimBar<T>& qb = left ? lb : rb;
+  const T s_k = left ? s_l : s_r;
+  // ---- reverse: physical flux of side k
+  const T m = q.r * q.u[0];
+  const T eh = q.e + q.p / q.r;
+  T mb = fb[0] + fb[1] * q.u[0] + fb[2] * q.u[1] + fb[3] * q.u[2] + fb[4] * eh;
+  qb.u[0] += fb[1] * m;
+  qb.u[1] += fb[2] * m;
+  qb.u[2] += fb[3] * m;
+  qb.p += fb[1] + fb[4] * m / q.r;
+  qb.e += fb[4] * m;
+  qb.r += -fb[4] * m * q.p / (q.r * q.r);
+  qb.r += mb * q.u[0];
+  qb.u[0] += mb * q.r;
+  T skb = T(0), smb = T(0);
+  if (star) {
+    const T v = q.u[0];
+    const T g = s_k - s_m;
+    const T rat = g == T(0) ? T(0) : s_k / g;
+    const T tt = g == T(0) ? T(0) : (s_k - v) / g;
+    const T dv = s_m - v;
+    T ratb = T(0), dvb = T(0), vb = T(0), ttb = T(0);
+    // f0 += rho dv rat
+    qb.r += fb[0] * dv * rat;
+    dvb += fb[0] * q.r * rat;
+    ratb += fb[0] * q.r * dv;
+    // f1 += rho s_k (tt s_m - v)
+    qb.r += fb[1] * s_k * (tt * s_m - v);
+    skb += fb[1] * q.r * (tt * s_m - v);
+    ttb += fb[1] * q.r * s_k * s_m;
+    smb += fb[1] * q.r * s_k * tt;
+    vb += -fb[1] * q.r * s_k;
+    // f2, f3 += rho dv u_i rat
+#pragma unroll
+    for (int i = 1; i < 3; ++i) {
+      const T f = fb[1 + i];
+      qb.r += f * dv * q.u[i] * rat;
+      dvb += f * q.r * q.u[i] * rat;
+      qb.u[i] += f * q.r * dv * rat;
+      ratb += f * q.r * dv * q.u[i];
+    }
+    // f4 += rho rat dv W, W = e + p/rho + (s_k - v) s_m
+    const T W = q.e + q.p / q.r + (s_k - v) * s_m;
+    qb.r += fb[4] * rat * dv * W;
+    ratb += fb[4] * q.r * dv * W;
+    dvb += fb[4] * q.r * rat * W;
+    const T Wb = fb[4] * q.r * rat * dv;
+    qb.e += Wb;
+    qb.p += Wb / q.r;
+    qb.r += -Wb * q.p / (q.r * q.r);
+    skb += Wb * s_m;
+    vb += -Wb * s_m;
+    smb += Wb * (s_k - v);
+    // dv = s_m - v
+    smb += dvb;
+    vb += -dvb;
+    if (g != T(0)) {
+      // rat = s_k / g, tt = (s_k - v) / g, g = s_k - s_m
+      const T ig = T(1) / g;
+      skb += ratb * (ig - s_k * ig * ig) + ttb * (ig - (s_k - v) * ig * ig);
+      smb += ratb * s_k * ig * ig + ttb * (s_k - v) * ig * ig;
+      vb += -ttb * ig;
+    }
+    qb.u[0] += vb;
+  }
+  // ---- wave speeds
+  T slb_ = left ? skb : T(0), srb_ = left ? T(0) : skb;
+  if (!clamp) {
+    const T numb = smb / dd;
+    const T ddb = -smb * num / (dd * dd);
+    lb.p -= numb;
+    rb.p += numb;
+    lb.r += numb * vl * (s_l - vl) + ddb * (s_l - vl);
+    lb.u[0] += numb * l.r * (s_l - T(2) * vl) - ddb * l.r;
+    slb_ += numb * l.r * vl + ddb * l.r;
+    rb.r += -numb * vr * (s_r - vr) - ddb * (s_r - vr);
+    rb.u[0] += -numb * r.r * (s_r - T(2) * vr) + ddb * r.r;
+    srb_ += -numb * r.r * vr - ddb * r.r;
+  }
+  T clb = T(0), crb = T(0), rcb = T(0), rub[3] = {T(0), T(0), T(0)};
+  if (lmin_a) {
+    lb.u[0] += slb_;
+    clb += -slb_;
+  } else {
+    rub[0] += slb_;
+    rcb += -slb_;
+  }
+  if (rmax_a) {
+    rb.u[0] += srb_;
+    crb += srb_;
+  } else {
+    rub[0] += srb_;
+    rcb += srb_;
+  }
+  const T hsb = dsqrt(rc, rcb) * gm1;
+  const T rhb = hsb;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) rub[i] += -hsb * ru[i];
+  T rlb = T(0), rrb = T(0), invb = T(0);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    rlb += rub[i] * l.u[i] * inv;
+    lb.u[i] += rub[i] * rl * inv;
+    rrb += rub[i] * r.u[i] * inv;
+    rb.u[i] += rub[i] * rr * inv;
+    invb += rub[i] * nu_[i];
+  }
+  rlb += rhb * l.h * inv;
+  lb.h += rhb * rl * inv;
+  rrb += rhb * r.h * inv;
+  rb.h += rhb * rr * inv;
+  invb += rhb * nh;
+  const T denb = -invb * inv * inv;
+  rlb += denb;
+  rrb += denb;
+  lb.r += dsqrt(rl, rlb);
+  rb.r += dsqrt(rr, rrb);
+  // c = sqrt(gamma p / rho)
+  const T cl2b = dsqrt(cl, clb), cr2b = dsqrt(cr, crb);
+  lb.p += cl2b * gam / l.r;
+  lb.r += -cl2b * gam * l.p / (l.r * l.r);
+  rb.p += cr2b * gam / r.r;
+  rb.r += -cr2b * gam * r.p / (r.r * r.r);
+}
+
+// Reverse of viscous_flux<T, 0> for the cotangent fb[1..4]. gab/gbb are the
+// cotangents of the tangential central differences ga[1][1], ga[1][0],
+// ga[2][2], ga[2][0] (and the same for b). Returns fb . F_visc / nu, the
+// viscous part's derivative with respect to nu (the flux is linear in nu).
+template <typename T>
+__device__ __forceinline__ T viscous_vjp(T ra, T rb, const T* ua, const T* ub,
+                                         T pa, T pb, const T* ga4,
+                                         const T* gb4, T h, T nu, T inv_pr,
+                                         const T* fb, T& rab, T& rbb, T* uab,
+                                         T* ubb, T& pab, T& pbb, T* gab,
+                                         T* gbb) {
+  const T R = K<T>::r_gas(), cp = K<T>::cp();
+  // forward (ga4/gb4 = g11, g10, g22, g20)
+  T bd[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) bd[c] = (ub[c] - ua[c]) / h;
+  const T g0 = bd[0], g1 = T(0.5) * (ga4[0] + gb4[0]),
+          g2 = T(0.5) * (ga4[2] + gb4[2]);
+  const T div = g0 + g1 + g2;
+  const T rf = T(0.5) * (ra + rb);
+  T s[3];
+  s[0] = bd[0] - T(1.0 / 3.0) * div;
+  s[1] = T(0.5) * (bd[1] + T(0.5) * (ga4[1] + gb4[1]));
+  s[2] = T(0.5) * (bd[2] + T(0.5) * (ga4[3] + gb4[3]));
+  T tau[3], uf[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    tau[c] = T(2) * rf * nu * s[c];
+    uf[c] = T(0.5) * (ua[c] + ub[c]);
+  }
+  const T ta = pa / (ra * R), tb = pb / (rb * R);
+  const T ka = inv_pr * cp * (nu * ra), kb = inv_pr * cp * (nu * rb);
+  const T kf = T(0.5) * (ka + kb);
+  const T q = -kf * ((tb - ta) / h);
+  const T dot = uf[0] * tau[0] + uf[1] * tau[1] + uf[2] * tau[2];
+  const T dnu = -(fb[1] * tau[0] + fb[2] * tau[1] + fb[3] * tau[2]) +
+                fb[4] * (q - dot);
+  // reverse
+  T taub[3], sb[3], bdb[3] = {T(0), T(0), T(0)};
+  T rfb = T(0);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    taub[c] = -fb[1 + c] - fb[4] * uf[c];
+    const T ufb = -fb[4] * tau[c];
+    uab[c] += T(0.5) * ufb;
+    ubb[c] += T(0.5) * ufb;
+    rfb += taub[c] * T(2) * nu * s[c];
+    sb[c] = taub[c] * T(2) * rf * nu;
+  }
+  const T qb = fb[4];
+  const T kfb = -qb * ((tb - ta) / h);
+  const T tbb = -qb * kf / h, tab = qb * kf / h;
+  rab += T(0.5) * kfb * inv_pr * cp * nu;
+  rbb += T(0.5) * kfb * inv_pr * cp * nu;
+  pab += tab / (ra * R);
+  rab += -tab * pa / (ra * ra * R);
+  pbb += tbb / (rb * R);
+  rbb += -tbb * pb / (rb * rb * R);
+  rab += T(0.5) * rfb;
+  rbb += T(0.5) * rfb;
+  const T divb = -sb[0] * T(1.0 / 3.0);
+  bdb[0] += sb[0] + divb;
+  bdb[1] += T(0.5) * sb[1];
+  bdb[2] += T(0.5) * sb[2];
+  gab[1] += T(0.25) * sb[1];
+  gbb[1] += T(0.25) * sb[1];
+  gab[3] += T(0.25) * sb[2];
+  gbb[3] += T(0.25) * sb[2];
+  gab[0] += T(0.5) * divb;
+  gbb[0] += T(0.5) * divb;
+  gab[2] += T(0.5) * divb;
+  gbb[2] += T(0.5) * divb;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    ubb[c] += bdb[c] / h;
+    uab[c] -= bdb[c] / h;
+  }
+  return nu > T(0) ? dnu / nu : T(0);
+}
+
+// ---------------------------------------------------------------------------
+// Kernels.
+// ---------------------------------------------------------------------------
+struct VjpArgs {
+  int nx, ny, nz, h;
+  long long sx, sz;
+  double dx, dy, dz;
+  const void* uk[5];
+  const void* lam[5];
+  void* prim[7];  // rho, u, v, w, e, p, h of uk, every cell
+  void* pbar[7];  // primitive cotangents, every cell
+  void* vout[5];  // conserved cotangents, every cell
+  const void* pe[3];
+  int has_pe;
+  int visc;
+  double nu, pr;
+  double beta;
+  int gravity_mask;
+  double g[3];
+  double* nu_bar;
+  int seg;  // faces per thread along a line
+};
+
+template <typename T>
+__device__ __forceinline__ T pe_of(const VjpArgs& a, int xa, int ya, int za) {
+  if (!a.has_pe) return T(0);
+  const T* px = static_cast<const T*>(a.pe[0]);
+  const T* py = static_cast<const T*>(a.pe[1]);
+  const T* pz = static_cast<const T*>(a.pe[2]);
+  return (-(px ? px[xa] : T(0)) - (py ? py[ya] : T(0))) - (pz ? pz[za] : T(0));
+}
+
+// Primitives of every cell (halos included).
+template <typename T>
+__global__ void vjp_prim_kernel(const VjpArgs a) {
+  const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h, nza = a.nz + 2 * a.h;
+  const long long n = (long long)nxa * nya * nza;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int ya = (int)(t % nya);
+    const int xa = (int)((t / nya) % nxa);
+    const int za = (int)(t / ((long long)nya * nxa));
+    const long long o = za * a.sz + xa * a.sx + ya;
+    T c[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) c[v] = static_cast<const T*>(a.uk[v])[o];
+    T u, v, w, e, p, hh;
+    cons_to_prim(c[0], c[1], c[2], c[3], c[4], pe_of<T>(a, xa, ya, za), u, v,
+                 w, e, p, hh);
+    const T pr[7] = {c[0], u, v, w, e, p, hh};
+#pragma unroll
+    for (int k = 0; k < 7; ++k) static_cast<T*>(a.prim[k])[o] = pr[k];
+  }
+}
+
+// Face VJPs along dim D. Thread = `seg` consecutive faces of one line along
+// D; a register window holds the 6-cell stencil primitives and their
+// cotangents, and a cell's cotangents are added to pbar once, when the
+// window leaves it.
+template <typename T, int D>
+__global__ void __launch_bounds__(128) vjp_face_kernel(const VjpArgs a) {
+  const int h = a.h;
+  const int n = D == 0 ? a.nx : (D == 1 ? a.ny : a.nz);
+  // Transverse axes (t1, t2) of the rotated frame: x:(y,z) y:(x,z) z:(x,y).
+  const int n1 = D == 0 ? a.ny : a.nx;
+  const int n2 = D == 2 ? a.ny : a.nz;
+  const long long st = D == 0 ? a.sx : (D == 1 ? 1 : a.sz);
+  const long long s1 = D == 0 ? 1 : a.sx;
+  const long long s2 = D == 2 ? 1 : a.sz;
+  const T hd = T(D == 0 ? a.dx : (D == 1 ? a.dy : a.dz));
+  const T h1 = T(D == 0 ? a.dy : a.dx);
+  const T h2 = T(D == 2 ? a.dy : a.dz);
+  const int nseg = (n + 1 + a.seg - 1) / a.seg;
+  // Thread index: the coordinate along y varies fastest (coalesced loads).
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long lines = (long long)n1 * n2;
+  // Threads past the last line take no faces but join the nu reduction.
+  const bool active = tid < lines * nseg;
+  int c1, c2, sg;
+  {
+    long long r = tid;
+    if (D == 2) {  // (t1, t2) = (x, y): y fastest
+      c2 = (int)(r % n2); r /= n2;
+      c1 = (int)(r % n1); r /= n1;
+    } else {  // t1 is y for D = 0; for D = 1, t1 = x
+      c1 = (int)(r % n1); r /= n1;
+      c2 = (int)(r % n2); r /= n2;
+    }
+    sg = (int)r;
+  }
+  const int i0 = active ? sg * a.seg : 0;
+  const int i1 = active ? min(i0 + a.seg, n + 1) : 0;
+  const long long base = (long long)(c1 + h) * s1 + (long long)(c2 + h) * s2;
+  const int vel[3] = {1 + D, D == 0 ? 2 : 1, D == 2 ? 2 : 3};
+  const T* P[7];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) P[k] = static_cast<const T*>(a.prim[k]);
+  // Rotated primitive of cell j (normal index with halo = j + h).
+  auto load = [&](int j, T* q) {
+    const long long o = base + (long long)(j + h) * st;
+    q[0] = P[0][o];
+    q[1] = P[vel[0]][o];
+    q[2] = P[vel[1]][o];
+    q[3] = P[vel[2]][o];
+    q[4] = P[4][o];
+    q[5] = P[5][o];
+    q[6] = P[6][o];
+  };
+  auto lam_at = [&](int j, T* lv) {
+    if (j < 0 || j >= n) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) lv[v] = T(0);
+      return;
+    }
+    const long long o = base + (long long)(j + h) * st;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) lv[v] = static_cast<const T*>(a.lam[v])[o];
+  };
+  auto flush = [&](int j, const T* b) {
+    const long long o = base + (long long)(j + h) * st;
+    atomicAdd(static_cast<T*>(a.pbar[0]) + o, b[0]);
+    atomicAdd(static_cast<T*>(a.pbar[vel[0]]) + o, b[1]);
+    atomicAdd(static_cast<T*>(a.pbar[vel[1]]) + o, b[2]);
+    atomicAdd(static_cast<T*>(a.pbar[vel[2]]) + o, b[3]);
+    atomicAdd(static_cast<T*>(a.pbar[4]) + o, b[4]);
+    atomicAdd(static_cast<T*>(a.pbar[5]) + o, b[5]);
+    atomicAdd(static_cast<T*>(a.pbar[6]) + o, b[6]);
+  };
+  // Window: cells i-3 .. i+2 for face i (face i-1/2 between i-1 and i).
+  T sw[6][7], ab[6][7];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+#pragma unroll
+    for (int v = 0; v < 7; ++v) ab[k][v] = T(0);
+  }
+#pragma unroll
+  for (int v = 0; v < 7; ++v) ab[5][v] = T(0);
+  T la[5], lb[5];
+  if (active) {
+#pragma unroll
+  for (int k = 0; k < 5; ++k) load(i0 - 3 + k, sw[k]);
+  }
+  lam_at(active ? i0 - 1 : -1, la);
+  const T scale = T(a.beta) / hd;
+  const T nu = T(a.nu), inv_pr = T(1.0 / a.pr);
+  const T gam = K<T>::gamma();
+  (void)gam;
+  T nub = T(0);
+  for (int i = i0; i < i1; ++i) {
+    load(i + 2, sw[5]);
+    lam_at(i, lb);
+    T fb[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) fb[v] = (lb[v] - la[v]) * scale;
+    // Rotate the flux cotangent to the rotated momentum order.
+    T fr[5];
+    fr[0] = fb[0];
+    fr[1] = fb[1 + D];
+    fr[2] = fb[1 + (D == 0 ? 1 : 0)];
+    fr[3] = fb[1 + (D == 2 ? 1 : 2)];
+    fr[4] = fb[4];
+    // Forward face states.
+    Prim<T> ql, qr;
+    {
+      T s[6];
+      T neg[7], pos[7];
+#pragma unroll
+      for (int v = 0; v < 7; ++v) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s[k] = sw[k][v];
+        neg[v] = weno5_right(s[0], s[1], s[2], s[3], s[4]);
+        pos[v] = weno5_left(s[1], s[2], s[3], s[4], s[5]);
+      }
+      ql.r = neg[0]; ql.u[0] = neg[1]; ql.u[1] = neg[2]; ql.u[2] = neg[3];
+      ql.e = neg[4]; ql.p = neg[5]; ql.h = neg[6];
+      qr.r = pos[0]; qr.u[0] = pos[1]; qr.u[1] = pos[2]; qr.u[2] = pos[3];
+      qr.e = pos[4]; qr.p = pos[5]; qr.h = pos[6];
+    }
+    int xa, ya, za;  // face cell b = i (pe at the face index)
+    {
+      const int jb = i + h;
+      if (D == 0) { xa = jb; ya = c1 + h; za = c2 + h; }
+      else if (D == 1) { ya = jb; xa = c1 + h; za = c2 + h; }
+      else { za = jb; xa = c1 + h; ya = c2 + h; }
+    }
+    const T pe = pe_of<T>(a, xa, ya, za);
+    PrimBar<T> lbar, rbar;
+    lbar.zero();
+    rbar.zero();
+    hllc_vjp<T>(ql, qr, pe, fr, lbar, rbar);
+    {
+      const T nb[7] = {lbar.r, lbar.u[0], lbar.u[1], lbar.u[2], lbar.e, lbar.p, lbar.h};
+      const T pb[7] = {rbar.r, rbar.u[0], rbar.u[1], rbar.u[2], rbar.e, rbar.p, rbar.h};
+#pragma unroll
+      for (int v = 0; v < 7; ++v) {
+        T s[6], sb[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s[k] = sw[k][v];
+        weno5_vjp<T, true>(s, nb[v], sb);
+        weno5_vjp<T, false>(s + 1, pb[v], sb + 1);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) ab[k][v] += sb[k];
+      }
+    }
+    if (a.visc) {
+      // Cells a = i-1 (window 2) and b = i (window 3) and the tangential
+      // neighbours of both for the cross derivatives.
+      const T* ca = sw[2];
+      const T* cb = sw[3];
+      const long long oa = base + (long long)(i - 1 + h) * st;
+      const long long ob = oa + st;
+      T ga4[4], gb4[4];
+      const T i2t1 = T(1) / (T(2) * h1), i2t2 = T(1) / (T(2) * h2);
+      // g11: t1 derivative of velocity t1; g10: of the normal velocity;
+      // g22 / g20 likewise along t2.
+      ga4[0] = (P[vel[1]][oa + s1] - P[vel[1]][oa - s1]) * i2t1;
+      ga4[1] = (P[vel[0]][oa + s1] - P[vel[0]][oa - s1]) * i2t1;
+      ga4[2] = (P[vel[2]][oa + s2] - P[vel[2]][oa - s2]) * i2t2;
+      ga4[3] = (P[vel[0]][oa + s2] - P[vel[0]][oa - s2]) * i2t2;
+      gb4[0] = (P[vel[1]][ob + s1] - P[vel[1]][ob - s1]) * i2t1;
+      gb4[1] = (P[vel[0]][ob + s1] - P[vel[0]][ob - s1]) * i2t1;
+      gb4[2] = (P[vel[2]][ob + s2] - P[vel[2]][ob - s2]) * i2t2;
+      gb4[3] = (P[vel[0]][ob + s2] - P[vel[0]][ob - s2]) * i2t2;
+      T rab = T(0), rbb = T(0), pab = T(0), pbb = T(0);
+      T uab[3] = {T(0), T(0), T(0)}, ubb[3] = {T(0), T(0), T(0)};
+      T gab[4] = {T(0), T(0), T(0), T(0)}, gbb[4] = {T(0), T(0), T(0), T(0)};
+      const T ua[3] = {ca[1], ca[2], ca[3]}, ub[3] = {cb[1], cb[2], cb[3]};
+      nub += viscous_vjp<T>(ca[0], cb[0], ua, ub, ca[5], cb[5], ga4, gb4, hd,
+                            nu, inv_pr, fr, rab, rbb, uab, ubb, pab, pbb, gab,
+                            gbb);
+      ab[2][0] += rab;
+      ab[3][0] += rbb;
+      ab[2][5] += pab;
+      ab[3][5] += pbb;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ab[2][1 + c] += uab[c];
+        ab[3][1 + c] += ubb[c];
+      }
+      // Tangential neighbours: cotangents of the central differences.
+      T* PB1 = static_cast<T*>(a.pbar[vel[1]]);
+      T* PB0 = static_cast<T*>(a.pbar[vel[0]]);
+      T* PB2 = static_cast<T*>(a.pbar[vel[2]]);
+      atomicAdd(PB1 + oa + s1, gab[0] * i2t1);
+      atomicAdd(PB1 + oa - s1, -gab[0] * i2t1);
+      atomicAdd(PB0 + oa + s1, gab[1] * i2t1);
+      atomicAdd(PB0 + oa - s1, -gab[1] * i2t1);
+      atomicAdd(PB2 + oa + s2, gab[2] * i2t2);
+      atomicAdd(PB2 + oa - s2, -gab[2] * i2t2);
+      atomicAdd(PB0 + oa + s2, gab[3] * i2t2);
+      atomicAdd(PB0 + oa - s2, -gab[3] * i2t2);
+      atomicAdd(PB1 + ob + s1, gbb[0] * i2t1);
+      atomicAdd(PB1 + ob - s1, -gbb[0] * i2t1);
+      atomicAdd(PB0 + ob + s1, gbb[1] * i2t1);
+      atomicAdd(PB0 + ob - s1, -gbb[1] * i2t1);
+      atomicAdd(PB2 + ob + s2, gbb[2] * i2t2);
+      atomicAdd(PB2 + ob - s2, -gbb[2] * i2t2);
+      atomicAdd(PB0 + ob + s2, gbb[3] * i2t2);
+      atomicAdd(PB0 + ob - s2, -gbb[3] * i2t2);
+    }
+    // Cell i-3 is complete for this thread: flush it and slide.
+    flush(i - 3, ab[0]);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+#pragma unroll
+      for (int v = 0; v < 7; ++v) {
+        sw[k][v] = sw[k + 1][v];
+        ab[k][v] = ab[k + 1][v];
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 7; ++v) ab[5][v] = T(0);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) la[v] = lb[v];
+  }
+  // Cells i1-3 .. i1+1 may still hold contributions.
+  if (active) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) flush(i1 - 3 + k, ab[k]);
+  }
+  if (a.visc && a.nu_bar) {
+    double m = double(nub);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      m += __shfl_xor_sync(0xffffffffu, m, off);
+    if ((threadIdx.x & 31) == 0 && m != 0.0) atomicAdd(a.nu_bar, m);
+  }
+}
+
+// Conserved cotangents of every cell from its primitive cotangents (the
+// reverse of cons_to_prim), plus the gravity source rho*G*g.
+template <typename T>
+__global__ void vjp_cell_kernel(const VjpArgs a) {
+  const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h, nza = a.nz + 2 * a.h;
+  const long long n = (long long)nxa * nya * nza;
+  const T gm1 = K<T>::gm1();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int ya = (int)(t % nya);
+    const int xa = (int)((t / nya) % nxa);
+    const int za = (int)(t / ((long long)nya * nxa));
+    const long long o = za * a.sz + xa * a.sx + ya;
+    T c[5], pb[7];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) c[v] = static_cast<const T*>(a.uk[v])[o];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) pb[k] = static_cast<const T*>(a.pbar[k])[o];
+    const T pe = pe_of<T>(a, xa, ya, za);
+    const T rho = c[0];
+    const T inv = T(1) / rho;
+    const T u[3] = {inv * c[1], inv * c[2], inv * c[3]};
+    const T e = inv * c[4];
+    const T eint = e - T(0.5) * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) - pe;
+    const T p = gm1 * rho * eint;
+    // h = e + p / rho
+    T eb = pb[4] + pb[6];
+    T pbb = pb[5] + pb[6] / rho;
+    T rb = pb[0] - pb[6] * p / (rho * rho);
+    // p = gm1 rho eint
+    rb += pbb * gm1 * eint;
+    const T eintb = pbb * gm1 * rho;
+    // eint = e - |u|^2/2 - pe
+    eb += eintb;
+    T ub[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) ub[i] = pb[1 + i] - eintb * u[i];
+    // e = inv E, u_i = inv m_i
+    T invb = eb * c[4];
+    T out[5];
+    out[4] = eb * inv;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      out[1 + i] = ub[i] * inv;
+      invb += ub[i] * c[1 + i];
+    }
+    rb += -invb * inv * inv;
+    // Gravity source on the momenta of interior cells.
+    const bool interior = xa >= a.h && xa < a.nx + a.h && ya >= a.h &&
+                          ya < a.ny + a.h && za >= a.h && za < a.nz + a.h;
+    if (a.gravity_mask && interior) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (a.gravity_mask & (1 << d))
+          rb += T(a.beta) * static_cast<const T*>(a.lam[1 + d])[o] *
+                K<T>::grav() * T(a.g[d]);
+    }
+    out[0] = rb;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) static_cast<T*>(a.vout[v])[o] = out[v];
+  }
+}
+
+// Reverse of one dim pass of the halo fill (swc_halo_fill) on vout: the
+// cotangent of every halo cell goes to the cell its value came from and the
+// halo cotangent is cleared (periodic: the wrapped interior layer; Neumann:
+// the edge cell; Dirichlet: nothing).
+struct VjpHalo {
+  int dim;
+  int nx, ny, nz, h;
+  long long sx, sz;
+  void* f[5];
+  SwcBC bc[5][2];
+};
+
+template <typename T>
+__global__ void vjp_halo_kernel(const VjpHalo a) {
+  const int ext[3] = {a.nx + 2 * a.h, a.ny + 2 * a.h, a.nz + 2 * a.h};
+  const long long stride[3] = {a.sx, 1, a.sz};
+  const int d = a.dim;
+  int ax_a, ax_b;
+  if (d == 0) { ax_a = 2; ax_b = 1; }
+  else if (d == 1) { ax_a = 2; ax_b = 0; }
+  else { ax_a = 0; ax_b = 1; }
+  const int na = ext[ax_a], nb = ext[ax_b];
+  const long long plane = (long long)na * nb;
+  const int n = ext[d] - 2 * a.h;
+  const long long total = plane * 2 * 5;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+       t < total; t += (long long)gridDim.x * blockDim.x) {
+    const long long pb = t % plane;
+    const int side = (int)((t / plane) % 2);
+    const int fi = (int)(t / (plane * 2));
+    const int ia = (int)(pb / nb), ib = (int)(pb % nb);
+    const long long base = ia * stride[ax_a] + ib * stride[ax_b];
+    const long long sd = stride[d];
+    T* f = static_cast<T*>(a.f[fi]);
+    const int kind = a.bc[fi][side].kind;
+    for (int l = 0; l < a.h; ++l) {
+      const long long o = side == 0 ? base + (long long)l * sd
+                                    : base + (long long)(n + a.h + l) * sd;
+      const T v = f[o];
+      if (kind == SWC_BC_NONE) continue;
+      f[o] = T(0);
+      if (kind == SWC_BC_PERIODIC) {
+        const long long src = side == 0 ? base + (long long)(l + n) * sd
+                                        : base + (long long)(a.h + l) * sd;
+        atomicAdd(f + src, v);
+      } else if (kind == SWC_BC_NEUMANN) {
+        const long long edge = side == 0 ? base + (long long)a.h * sd
+                                         : base + (long long)(n + a.h - 1) * sd;
+        atomicAdd(f + edge, v);
+      }
+    }
+  }
+}
+
+template <typename T>
+int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
+  const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h, nza = a.nz + 2 * a.h;
+  const long long cells = (long long)nxa * nya * nza;
+  const int pt = 256;
+  const unsigned pblocks = (unsigned)std::min<long long>((cells + pt - 1) / pt, 148 * 16);
+  vjp_prim_kernel<T><<<pblocks, pt, 0, s>>>(a);
+  note_launch();
+  for (int k = 0; k < 7; ++k) {
+    cudaError_t e = cudaMemsetAsync(a.pbar[k], 0, (size_t)(a.sz * nza) * sizeof(T), s);
+    if (e != cudaSuccess) return record_error(SWC_ERR_LAUNCH, "memset: %s", cudaGetErrorString(e));
+  }
+  const int ft = 128;
+  for (int D = 0; D < 3; ++D) {
+    const int n = D == 0 ? a.nx : (D == 1 ? a.ny : a.nz);
+    const int n1 = D == 0 ? a.ny : a.nx;
+    const int n2 = D == 2 ? a.ny : a.nz;
+    const long long nseg = (n + 1 + a.seg - 1) / a.seg;
+    const long long threads = (long long)n1 * n2 * nseg;
+    const unsigned blocks = (unsigned)((threads + ft - 1) / ft);
+    if (D == 0) vjp_face_kernel<T, 0><<<blocks, ft, 0, s>>>(a);
+    else if (D == 1) vjp_face_kernel<T, 1><<<blocks, ft, 0, s>>>(a);
+    else vjp_face_kernel<T, 2><<<blocks, ft, 0, s>>>(a);
+    note_launch();
+  }
+  vjp_cell_kernel<T><<<pblocks, pt, 0, s>>>(a);
+  note_launch();
+  for (int d = 2; d >= 0; --d) {
+    VjpHalo hh;
+    memset(&hh, 0, sizeof(hh));
+    hh.dim = d;
+    hh.nx = a.nx; hh.ny = a.ny; hh.nz = a.nz; hh.h = a.h;
+    hh.sx = a.sx; hh.sz = a.sz;
+    for (int v = 0; v < 5; ++v) {
+      hh.f[v] = a.vout[v];
+      const SwcBC& lo = bcs[v].side[d][0];
+      const SwcBC& hi = bcs[v].side[d][1];
+      hh.bc[v][0] = lo;
+      hh.bc[v][1] = hi;
+      if (lo.kind == SWC_BC_PERIODIC || hi.kind == SWC_BC_PERIODIC)
+        hh.bc[v][0].kind = hh.bc[v][1].kind = SWC_BC_PERIODIC;
+    }
+    const int ext[3] = {nxa, nya, nza};
+    const long long total = (long long)ext[(d + 1) % 3] * ext[(d + 2) % 3] * 10;
+    const unsigned hb = (unsigned)std::min<long long>((total + 255) / 256, 148 * 16);
+    vjp_halo_kernel<T><<<hb, 256, 0, s>>>(hh);
+    note_launch();
+  }
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? SWC_OK
+                          : record_error(SWC_ERR_LAUNCH, "stage vjp: %s",
+                                         cudaGetErrorString(e));
+}
+
+}  // namespace
+}  // namespace swc
+
+extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
+                                const SwcFieldBC* bcs, const void* const* uk,
+                                const void* const* lam, double beta,
+                                void* const* vout, double* nu_bar,
+                                void* const* scratch, void* stream) {
+  using namespace swc;
+  int st = check_grid(grid);
+  if (st) return st;
+  if (!sc || !bcs || !uk || !lam || !vout || !scratch)
+    return record_error(SWC_ERR_ARG, "stage vjp: NULL argument");
+  if (sc->dtype != SWC_F32 && sc->dtype != SWC_F64)
+    return record_error(SWC_ERR_ARG, "bad dtype %d", sc->dtype);
+  if (sc->interp != SWC_WENO5 || sc->riemann != SWC_HLLC || sc->nscalars != 0)
+    return record_error(SWC_ERR_UNSUPPORTED,
+                        "the stage adjoint covers WENO5 + HLLC without "
+                        "transported scalars");
+  if (grid->halo < 3)
+    return record_error(SWC_ERR_ARG, "halo_width %d is too small (needs 3)",
+                        grid->halo);
+  for (int v = 0; v < 5; ++v) {
+    if (!uk[v] || !lam[v] || !vout[v])
+      return record_error(SWC_ERR_ARG, "stage vjp: NULL field %d", v);
+    if (bcs[v].via_primitive)
+      return record_error(SWC_ERR_UNSUPPORTED,
+                          "the stage adjoint does not cover primitive BCs");
+  }
+  for (int k = 0; k < 14; ++k)
+    if (!scratch[k]) return record_error(SWC_ERR_ARG, "NULL scratch field %d", k);
+  VjpArgs a;
+  memset(&a, 0, sizeof(a));
+  a.nx = grid->nx; a.ny = grid->ny; a.nz = grid->nz; a.h = grid->halo;
+  a.sx = grid->sx; a.sz = grid->sz;
+  a.dx = grid->dx; a.dy = grid->dy; a.dz = grid->dz;
+  for (int v = 0; v < 5; ++v) {
+    a.uk[v] = uk[v];
+    a.lam[v] = lam[v];
+    a.vout[v] = vout[v];
+  }
+  for (int k = 0; k < 7; ++k) {
+    a.prim[k] = scratch[k];
+    a.pbar[k] = scratch[7 + k];
+  }
+  for (int d = 0; d < 3; ++d) {
+    a.pe[d] = sc->pe_axis[d];
+    if (sc->pe_axis[d]) a.has_pe = 1;
+    a.g[d] = sc->g[d];
+  }
+  a.visc = sc->diffusion ? 1 : 0;
+  a.nu = sc->nu;
+  a.pr = sc->pr > 0 ? sc->pr : 1.0;
+  a.beta = beta;
+  a.gravity_mask = sc->gravity_mask;
+  a.nu_bar = nu_bar;
+  a.seg = 16;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return sc->dtype == SWC_F32 ? launch_vjp<float>(a, bcs, s)
+                              : launch_vjp<double>(a, bcs, s);
+}

@@ -1,0 +1,172 @@
+"""GPU: the discrete adjoint of whole runs (swc_rk_stage_vjp through
+swirlc_b200.adjoint) against float64 central differences of the same runs,
+h = 1e-6 along seeded random directions in (initial state, nu), as the
+reference's gradient check prescribes; plus the autograd front end."""
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ('rho', 'rho_u', 'rho_v', 'rho_w', 'rho_e')
+
+
+def _setup(user_cfg, state, dtype=torch.float64, nu=None):
+  from swirlc_b200 import engine
+  from swirlc_b200.core import parameter
+  from swirlc_b200.physics import physics_models
+  cfg = parameter.SwirlCParameters(user_cfg)
+  f = [torch.tensor(state[k], dtype=dtype, device='cuda') for k in NAMES]
+  s = engine.Solver(cfg, physics_models.PhysicsModels(cfg), f[0].shape, dtype)
+  if nu is not None:
+    s.scheme.nu = nu
+  return cfg, s, f
+
+
+def _loss(s, fields):
+  from swirlc_b200 import adjoint
+  return adjoint.vorticity_energy(fields, s.hw, s.grid.dx, s.grid.dy,
+                                  s.grid.dz)
+
+
+def _linear_loss(weights):
+  """Seeded linear functional of the final state, balanced per field."""
+  def loss(s, fields):
+    return sum((w * f).sum() for w, f in zip(weights, fields))
+  return loss
+
+
+def _loss_grad(s, fields, loss=_loss):
+  x = [f.detach().clone().requires_grad_(True) for f in fields]
+  j = loss(s, x)
+  g = torch.autograd.grad(j, x, allow_unused=True)
+  return [torch.zeros_like(f) if gi is None else gi for f, gi in zip(fields, g)]
+
+
+def _check_fd(user_cfg, state, steps, k, dts, ndir, seed=0, tol=1e-6,
+              with_nu=True, linear=False):
+  from swirlc_b200 import adjoint
+  cfg, s, f = _setup(user_cfg, state)
+  loss = _loss
+  if linear:
+    rng_w = np.random.default_rng(100 + seed)
+    hw = s.hw
+    ws = []
+    for x in f:
+      w = torch.zeros_like(x)
+      inner_ = (slice(hw, -hw),) * 3
+      scale = float(x[inner_].abs().max()) or 1.0
+      w[inner_] = torch.tensor(rng_w.standard_normal(x[inner_].shape) / scale,
+                               dtype=x.dtype, device='cuda')
+      ws.append(w)
+    loss = _linear_loss(ws)
+  nu0 = float(s.scheme.nu)
+  run = adjoint.RunAdjoint(s, checkpoint_every=k)
+  out = run.run(f, dts)
+  grad, nub = run.backward(_loss_grad(s, out, loss))
+  hw = s.hw
+  inner = (slice(hw, -hw),) * 3
+  rng = np.random.default_rng(seed)
+  h = 1e-6
+  worst = 0.0
+  for _ in range(ndir):
+    d = []
+    for x in f:
+      scale = float(x[inner].abs().max()) or 1.0
+      dd = torch.zeros_like(x)
+      dd[inner] = torch.tensor(rng.standard_normal(x[inner].shape) * scale,
+                               dtype=x.dtype, device='cuda')
+      d.append(dd)
+    dnu = float(rng.standard_normal()) * nu0 if with_nu else 0.0
+    js = []
+    for sgn in (1.0, -1.0):
+      s.scheme.nu = nu0 + sgn * h * dnu
+      r2 = adjoint.RunAdjoint(s, checkpoint_every=k)
+      o2 = r2.run([x + sgn * h * dx for x, dx in zip(f, d)], dts)
+      js.append(float(loss(s, o2)))
+    s.scheme.nu = nu0
+    fd = (js[0] - js[1]) / (2 * h)
+    ad = sum(float((g[inner] * dx[inner]).sum()) for g, dx in zip(grad, d))
+    ad += nub * dnu
+    rel = abs(fd - ad) / max(abs(fd), abs(ad), 1e-30)
+    worst = max(worst, rel)
+    assert rel <= tol, (fd, ad, rel)
+  return worst
+
+
+def test_kh_viscous_periodic_gradient_matches_fd():
+  from swirlc_b200 import configs
+  cfg, state = configs.kelvin_helmholtz(n=12, nu=1e-2, dtype=np.float64)
+  dts = [2e-3] * 7
+  _check_fd(cfg, state, 7, 3, dts, ndir=16, seed=0)
+
+
+def test_sod_neumann_walls_gradient_matches_fd():
+  from swirlc_b200 import configs
+  cfg, state = configs.sod(n=24, ny=4, nz=4, dtype=np.float64)
+  dts = [1.5e-3] * 5
+  _check_fd(cfg, state, 5, 2, dts, ndir=8, seed=1, with_nu=False, linear=True)
+
+
+def test_gravity_dirichlet_walls_gradient_matches_fd():
+  from swirlc_b200 import configs
+  cfg, state = configs.buoyant_bubble(nx=8, ny=6, nz=12, dtype=np.float64)
+  cfg = dict(cfg, interpolation_scheme='WENO_5', numeric_flux_scheme='HLLC',
+             include_diffusion=True,
+             transport_parameters={'nu': 1e-1, 'pr': 0.7})
+  dts = [5e-3] * 4
+  _check_fd(cfg, state, 4, 2, dts, ndir=8, seed=2, linear=True)
+
+
+def test_autograd_front_end_matches_reverse_sweep():
+  from swirlc_b200 import adjoint, configs
+  cfg, state = configs.kelvin_helmholtz(n=12, nu=1e-2, dtype=np.float64)
+  _, s, f = _setup(cfg, state)
+  dts = [2e-3] * 4
+  run = adjoint.RunAdjoint(s, checkpoint_every=2)
+  x = [t.clone().requires_grad_(True) for t in f]
+  nu = torch.tensor(float(s.scheme.nu), dtype=torch.float64,
+                    requires_grad=True)
+  out = adjoint.simulate(run, x, dts, nu)
+  loss = _loss(s, out)
+  loss.backward()
+  run2 = adjoint.RunAdjoint(s, checkpoint_every=4)
+  o2 = run2.run(f, dts)
+  g2, nub2 = run2.backward(_loss_grad(s, o2))
+  hw = s.hw
+  inner = (slice(hw, -hw),) * 3
+  for a, b in zip(x, g2):
+    torch.testing.assert_close(a.grad[inner], b[inner], rtol=1e-12, atol=0)
+  assert float(nu.grad) == pytest.approx(nub2, rel=1e-12)
+
+
+def test_float32_adjoint_agrees_with_float64():
+  from swirlc_b200 import adjoint, configs
+  cfg, state = configs.kelvin_helmholtz(n=16, nu=1e-2, dtype=np.float64)
+  dts = [2e-3] * 4
+  grads = {}
+  for dt_ in (torch.float32, torch.float64):
+    _, s, f = _setup(cfg, state, dt_)
+    run = adjoint.RunAdjoint(s, checkpoint_every=2)
+    o = run.run(f, dts)
+    g, nub = run.backward(_loss_grad(s, o))
+    grads[dt_] = ([x.double() for x in g], nub)
+  hw = 3
+  inner = (slice(hw, -hw),) * 3
+  for a, b in zip(grads[torch.float32][0], grads[torch.float64][0]):
+    err = float((a[inner] - b[inner]).norm() / b[inner].norm())
+    assert err <= 1e-3, err
+  assert grads[torch.float32][1] == pytest.approx(grads[torch.float64][1],
+                                                  rel=1e-3)
+
+
+def test_adjoint_rejects_unsupported_schemes():
+  from swirlc_b200 import adjoint, configs
+  cfg, state = configs.sod(n=24, ny=4, nz=4, dtype=np.float64)
+  cfg = dict(cfg, interpolation_scheme='MUSCL')
+  _, s, f = _setup(cfg, state)
+  run = adjoint.RunAdjoint(s, checkpoint_every=2)
+  o = run.run(f, [1e-3])
+  with pytest.raises(NotImplementedError):
+    run.backward(_loss_grad(s, o))
