@@ -6,7 +6,7 @@ unit cube of 256^3 interior cells, float32, WENO5-JS + HLLC + viscous
 Seeded synthetic initial condition (swirlc_b200.configs.kelvin_helmholtz).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload kh256|riemann_batch]
+                  [--workload kh256|riemann_batch|adjoint]
 
 Under torchrun each rank advances its own 256^3 domain (weak scaling,
 replicas; the halo exchange of a decomposed domain is a separate path).
@@ -473,6 +473,171 @@ def run_batch(args):
     dist.destroy_process_group()
 
 
+ADJ_METRIC = ('adjoint/forward time ratio, KH 128^3 fp32 WENO5+HLLC+viscous, '
+              '200 SSP-RK3 steps, checkpoints every 20')
+
+
+def _adjoint_fd_check(n, steps, k, ndir=16, h=1e-6):
+  """Float64 central differences of the vorticity energy along seeded random
+  directions in (initial velocity, nu), against the adjoint gradient."""
+  import torch
+  from swirlc_b200 import adjoint, configs, engine
+  from swirlc_b200.core import parameter
+  from swirlc_b200.physics import physics_models
+  user_cfg, state = configs.kelvin_helmholtz(n=n, dtype=np.float64)
+  cfg = parameter.SwirlCParameters(user_cfg)
+  names = ('rho', 'rho_u', 'rho_v', 'rho_w', 'rho_e')
+  f = [torch.tensor(state[k_], dtype=torch.float64, device='cuda') for k_ in names]
+  s = engine.Solver(cfg, physics_models.PhysicsModels(cfg), f[0].shape,
+                    torch.float64)
+  st = engine.Stepper(s, [x.clone() for x in f], dt=cfg.dt, cfl=cfg.cfl)
+  dts = []
+  for _ in range(steps):
+    st.step(1)
+    dts.append(float(st.clock[1].item()))
+  hw = s.hw
+  inner = (slice(hw, -hw),) * 3
+  rho = f[0]
+  # Control: the initial velocity (its seeded perturbation included) at
+  # fixed rho and p.
+  vel = [f[i] / rho for i in (1, 2, 3)]
+  p0 = 0.4 * (f[4] - 0.5 * rho * (vel[0] ** 2 + vel[1] ** 2 + vel[2] ** 2))
+
+  def state_of(v):
+    ke = 0.5 * rho * (v[0] ** 2 + v[1] ** 2 + v[2] ** 2)
+    return [rho, rho * v[0], rho * v[1], rho * v[2], p0 / 0.4 + ke]
+
+  def loss(out):
+    return adjoint.vorticity_energy(out, hw, s.grid.dx, s.grid.dy, s.grid.dz)
+
+  nu0 = float(s.scheme.nu)
+  run = adjoint.RunAdjoint(s, checkpoint_every=k)
+  v = [x.clone().requires_grad_(True) for x in vel]
+  nu = torch.tensor(nu0, dtype=torch.float64, requires_grad=True)
+  out = adjoint.simulate(run, state_of(v), dts, nu)
+  j = loss(out)
+  j.backward()
+  gv = [x.grad for x in v]
+  gnu = float(nu.grad)
+  rng = np.random.default_rng(0)
+  rels = []
+  for _ in range(ndir):
+    d = []
+    for x in vel:
+      dd = torch.zeros_like(x)
+      dd[inner] = torch.tensor(rng.standard_normal(x[inner].shape), dtype=x.dtype,
+                               device='cuda')
+      d.append(dd)
+    dnu = float(rng.standard_normal()) * nu0
+    js = []
+    for sgn in (1.0, -1.0):
+      s.scheme.nu = nu0 + sgn * h * dnu
+      r2 = adjoint.RunAdjoint(s, checkpoint_every=k)
+      o2 = r2.run(state_of([a + sgn * h * b for a, b in zip(vel, d)]), dts)
+      js.append(float(loss(o2)))
+    s.scheme.nu = nu0
+    fd = (js[0] - js[1]) / (2 * h)
+    ad = sum(float((g[inner] * b[inner]).sum()) for g, b in zip(gv, d)) + gnu * dnu
+    rels.append(abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
+  return {'directions': ndir, 'h': h, 'dtype': 'f64', 'grid': f'{n}^3',
+          'steps': steps, 'median_rel_err': float(np.median(rels)),
+          'max_rel_err': float(np.max(rels)), 'loss': float(j)}
+
+
+def run_adjoint(args):
+  """Config 5: the discrete adjoint of 200 KH steps at 128^3 (fp32)."""
+  import torch
+  from swirlc_b200 import _native as nat
+  from swirlc_b200 import adjoint, configs, engine
+  from swirlc_b200.core import parameter
+  from swirlc_b200.physics import physics_models
+  rank, world, local = _env_rank()
+  torch.cuda.set_device(local)
+  n, steps, k = args.adj_n, args.adj_steps, 20
+  user_cfg, state = configs.kelvin_helmholtz(n=n, seed=rank)
+  cfg = parameter.SwirlCParameters(user_cfg)
+  names = ('rho', 'rho_u', 'rho_v', 'rho_w', 'rho_e')
+  f = [torch.tensor(state[k_], device='cuda') for k_ in names]
+  s = engine.Solver(cfg, physics_models.PhysicsModels(cfg), f[0].shape,
+                    torch.float32)
+  st = engine.Stepper(s, [x.clone() for x in f], dt=cfg.dt, cfl=cfg.cfl)
+  dts = []
+  for _ in range(steps):
+    st.step(1)
+    dts.append(float(st.clock[1].item()))
+  del st
+  run = adjoint.RunAdjoint(s, checkpoint_every=k, steps=steps)
+
+  def loss(out):
+    return adjoint.vorticity_energy(out, s.hw, s.grid.dx, s.grid.dy, s.grid.dz)
+
+  def loss_grad(out):
+    x = [o.detach().clone().requires_grad_(True) for o in out]
+    g = torch.autograd.grad(loss(x), x, allow_unused=True)
+    return [torch.zeros_like(o) if gi is None else gi for o, gi in zip(out, g)]
+
+  # Warm-up on a short run (kernel variants loaded, allocator warm).
+  for _ in range(max(1, args.warmup - 2)):
+    o0 = run.run(f, dts[:k])
+    run.backward(loss_grad(o0))
+  torch.cuda.synchronize()
+  sampler = ClockSampler(local)
+  sampler.start()
+  e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+  e[0].record()
+  out = run.run(f, dts)
+  e[1].record()
+  c0 = nat.launch_count()
+  g_in, nub = run.backward(loss_grad(out))
+  e[2].record()
+  torch.cuda.synchronize()
+  clocks = sampler.stop()
+  launches = nat.launch_count() - c0
+  fwd_ms, bwd_ms = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+  cells = n ** 3
+  # The same run keeping every stage state (no recomputation in the sweep).
+  del run
+  torch.cuda.empty_cache()
+  run_all = adjoint.RunAdjoint(s, checkpoint_every=0, steps=steps)
+  e2 = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+  e2[0].record()
+  out_all = run_all.run(f, dts)
+  e2[1].record()
+  run_all.backward(loss_grad(out_all))
+  e2[2].record()
+  torch.cuda.synchronize()
+  fwd_all, bwd_all = e2[0].elapsed_time(e2[1]), e2[1].elapsed_time(e2[2])
+  del run_all, out_all
+  torch.cuda.empty_cache()
+  fd = _adjoint_fd_check(n, steps, k) if args.fd_check else None
+  if rank == 0:
+    line = {
+        'metric': ADJ_METRIC, 'value': bwd_ms / fwd_ms, 'unit': 'ratio',
+        'n_gpus': world, 'steps': steps, 'warmup': args.warmup,
+        'ms_per_step': bwd_ms / steps, 'higher_is_better': False,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+        'data': 'synthetic (seeded KH initial condition)',
+        'config': {'workload': f'kelvin_helmholtz {n}^3 fp32 WENO5+HLLC+viscous '
+                               f'nu=1e-4, {steps} SSP-RK3 steps (device-CFL '
+                               'dt sequence, held fixed), checkpoints every '
+                               f'{k}, loss = vorticity energy',
+                   'cells': cells, 'l2_flush': 'inputs larger than L2'},
+        'forward_ms': fwd_ms, 'backward_ms': bwd_ms,
+        'forward_cell_updates_per_s': cells * steps / (fwd_ms / 1e3),
+        'target': 'backward <= 3 x forward',
+        'stored_stages': {'forward_ms': fwd_all, 'backward_ms': bwd_all,
+                          'ratio': bwd_all / fwd_all,
+                          'how': 'checkpoint_every=0: every stage state kept '
+                                 f'({steps} x 3 states, buffers allocated '
+                                 'once by the runner, no recomputation)'},
+        'grad_nu': nub,
+        'gpu_launches_backward': launches,
+        'fd_check': fd,
+        'clocks': clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_profile(args):
   """Eager RK3 steps of the workload, no timing: the command ncu captures."""
   import torch
@@ -596,8 +761,13 @@ def main():
   ap.add_argument('--n', type=int, default=N_CELLS_EDGE)
   ap.add_argument('--cpu-sample', type=int, default=96)
   ap.add_argument('--no-cpu-baseline', action='store_true')
+  ap.add_argument('--adj-n', type=int, default=128)
+  ap.add_argument('--adj-steps', type=int, default=200)
+  ap.add_argument('--fd-check', action='store_true',
+                  help='adjoint workload: add the float64 16-direction '
+                       'central-difference check at full size')
   ap.add_argument('--workload', default='kh256',
-                  choices=['kh256', 'riemann_batch'],
+                  choices=['kh256', 'riemann_batch', 'adjoint'],
                   help='kh256: the headline 256^3 Kelvin-Helmholtz step; '
                        'riemann_batch: 64 batched Riemann problems')
   ap.add_argument('--profile-steps', type=int, default=0,
@@ -613,6 +783,8 @@ def main():
     run_reference(args)
   elif args.workload == 'riemann_batch':
     run_batch(args)
+  elif args.workload == 'adjoint':
+    run_adjoint(args)
   else:
     run_ours(args)
 

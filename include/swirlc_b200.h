@@ -254,21 +254,25 @@ int swc_batch_step(const SwcScheme* scheme, int32_t order, int32_t nmembers,
                    const SwcBatchMember* members, void* stream);
 
 /* Reverse mode of one fused stage for WENO5 + HLLC (+ viscous), no
- * transported scalars, on the halo-filled state `uk` of that stage:
- *   vout   = beta * H^T J_L(H uk)^T lam   (H: halo fill with `bcs`),
- *   nu_bar += beta * lam . dL/dnu          (device double; may be NULL),
- * where L is the right-hand side the stage adds (compressible_navier_stokes
- * .py:68-268) and lam the cotangent of the stage output (interior cells;
- * its halos are not read). A stage out = A*u0 + B*(uk + dt*L(uk)) (rk3.py:
- * 87-120) passes beta = B*dt; its uk cotangent is B*lam + vout on the
- * interior, its u0 cotangent A*lam. vout is written on every cell (halos
- * hold zero afterwards for periodic, Dirichlet and Neumann BCs). `scratch`
- * is 14 caller buffers of the shape of uk. The reference differentiates this
- * path with TF's GradientTape; this is its discrete adjoint. */
+ * transported scalars, on the halo-filled state `uk` of that stage. On the
+ * interior cells
+ *   vout = alpha*lam + c1*x1 + c2*x2 + beta * H^T J_L(H uk)^T lam,
+ * (x1, x2 may be NULL; H: halo fill with `bcs`), halos of vout set to 0,
+ * and nu_bar (device double; may be NULL) += beta * lam . dL/dnu, where L
+ * is the right-hand side a stage adds (compressible_navier_stokes.py:
+ * 68-268) and lam the cotangent of the stage output (its halos are not
+ * read). A stage out = A*u0 + B*(uk + dt*L(uk)) (rk3.py:87-120) has the uk
+ * cotangent B*lam + B*dt*H^T J^T lam (alpha = B, beta = B*dt) and the u0
+ * cotangent A*lam, which x1 / x2 let the caller fold in. vout must not alias
+ * uk, lam, x1 or x2. `scratch` is 14 caller buffers of the shape of uk. The
+ * reference differentiates this path with TF's GradientTape; this is its
+ * discrete adjoint. */
 int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* scheme,
                      const SwcFieldBC* bcs, const void* const* uk,
-                     const void* const* lam, double beta, void* const* vout,
-                     double* nu_bar, void* const* scratch, void* stream);
+                     const void* const* lam, double alpha, double beta,
+                     const void* const* x1, double c1, const void* const* x2,
+                     double c2, void* const* vout, double* nu_bar,
+                     void* const* scratch, void* stream);
 
 /* dtmin_out <- min(dtmin_out, min over interior cells and dims of
  * delta_d / (|u_d| + c)), c = sqrt(gamma p / rho) (CFL rule of the

@@ -165,7 +165,7 @@ def load(require_cuda: bool = True) -> ctypes.CDLL:
       lib.swc_rk_stage_vjp.argtypes = [ctypes.POINTER(SwcGrid),
                                        ctypes.POINTER(SwcScheme),
                                        ctypes.POINTER(SwcFieldBC), pp, pp, dbl,
-                                       pp, vp, pp, vp]
+                                       dbl, pp, dbl, pp, dbl, pp, vp, pp, vp]
       lib.swc_batch_step.argtypes = [ctypes.POINTER(SwcScheme), i32, i32,
                                      ctypes.POINTER(SwcBatchMember), vp]
       lib.swc_rk_step_noalloc.argtypes = [ctypes.POINTER(SwcGrid),

@@ -34,17 +34,21 @@ class RunAdjoint:
 
   Args:
     solver: an `engine.Solver` (WENO5 + HLLC, optionally viscous).
-    checkpoint_every: steps between stored states.
+    checkpoint_every: steps between stored states; 0 keeps every step's
+      stage states during the forward run instead (no recomputation in the
+      backward sweep; memory: steps x 3 states of the fields).
     scheme: 'rk3' or 'rk2'.
+    steps: when known, the run length, so that the stage buffers (reused by
+      every run and sweep) are allocated here rather than during the run.
   """
 
   def __init__(self, solver: engine.Solver, checkpoint_every: int = 20,
-               scheme: str = 'rk3'):
+               scheme: str = 'rk3', steps: int = 0):
     if scheme not in ('rk3', 'rk2'):
       raise NotImplementedError(f'"{scheme}" is not implemented as an '
                                 '"time_integration_scheme".')
-    if checkpoint_every < 1:
-      raise ValueError('checkpoint_every must be >= 1.')
+    if checkpoint_every < 0:
+      raise ValueError('checkpoint_every must be >= 0.')
     self.s = solver
     self.k = int(checkpoint_every)
     self.order = 3 if scheme == 'rk3' else 2
@@ -52,31 +56,53 @@ class RunAdjoint:
     self.dts: List[float] = []
     self._scratch = [torch.empty(solver.shape, dtype=solver.dtype,
                                  device=solver.device) for _ in range(14)]
-    self._vout = solver.new_fields(zero=True)
+    self._g = [solver.new_fields(zero=True) for _ in range(4)]
     self._nu_bar = torch.zeros(1, dtype=torch.float64, device=solver.device)
+    self._pool: List = []  # per-step stage buffers, reused
+    self._tmp = None       # stage buffers of steps that keep nothing
+    self._u = None         # working state of the recomputed segment
+    self._ckpt_pool: List = []  # checkpoint states, reused
+    if steps:
+      self._reserve(steps if self.k == 0 else min(self.k, steps))
+      if self.k:
+        self._reserve_checkpoints((steps + self.k - 1) // self.k)
 
   # ------------------------------------------------------------- forward
-  def _step(self, u, dt, keep: Optional[list] = None):
-    """One step in place on u with fixed dt; `keep` receives the halo-filled
-    stage states (u, u1, u2) when given."""
+  def _new_buffers(self):
+    n = 3 if self.order == 3 else 2
+    return tuple(self.s.new_fields(zero=False) for _ in range(n))
+
+  def _reserve(self, n: int) -> None:
+    while len(self._pool) < n:
+      self._pool.append(self._new_buffers())
+
+  def _reserve_checkpoints(self, n: int) -> None:
+    while len(self._ckpt_pool) < n:
+      self._ckpt_pool.append(self.s.new_fields(zero=False))
+
+  def _step(self, u, dt, buf=None):
+    """One step in place on u with fixed dt; the halo-filled stage states
+    (u, u1, u2) are left in `buf` (scratch buffers when None)."""
     s = self.s
+    if buf is None:
+      if self._tmp is None:
+        self._tmp = self._new_buffers()
+      buf = self._tmp
     dtt = s.dt_tensor(dt)
     s.fill_halos(u)
-    u0 = [f.clone() for f in u]
-    w1 = s.new_fields(zero=False)
+    u0, w1 = buf[0], buf[1]
+    for a, b in zip(u0, u):
+      a.copy_(b)
     s.stage(u0, None, w1, nat.SWC_OUT_EULER, dt=dtt)
     s.fill_halos(w1)
     if self.order == 3:
-      w2 = s.new_fields(zero=False)
+      w2 = buf[2]
       s.stage(w1, u0, w2, nat.SWC_OUT_CONVEX, 0.75, 0.25, dt=dtt)
       s.fill_halos(w2)
       s.stage(w2, u0, u, nat.SWC_OUT_CONVEX, 1.0 / 3.0, 2.0 / 3.0, dt=dtt)
-      if keep is not None:
-        keep.append((u0, w1, w2))
     else:
       s.stage(w1, u0, u, nat.SWC_OUT_AVERAGE, 0.5, 0.0, dt=dtt)
-      if keep is not None:
-        keep.append((u0, w1))
+    return buf
 
   def run(self, fields: Sequence[torch.Tensor],
           dts: Sequence[float]) -> List[torch.Tensor]:
@@ -85,31 +111,49 @@ class RunAdjoint:
     self.dts = [float(d) for d in dts]
     u = [f.detach().clone() for f in fields]
     self.checkpoints = []
+    if self.k == 0:
+      self._reserve(len(self.dts))
     for i, dt in enumerate(self.dts):
+      if self.k == 0:
+        self._step(u, dt, self._pool[i])
+        continue
       if i % self.k == 0:
-        self.checkpoints.append([f.clone() for f in u])
+        c = i // self.k
+        self._reserve_checkpoints(c + 1)
+        for a, b in zip(self._ckpt_pool[c], u):
+          a.copy_(b)
+        self.checkpoints.append(self._ckpt_pool[c])
       self._step(u, dt)
+    if self.k == 0:
+      self.checkpoints = [None]
     self.s.fill_halos(u)
     return u
 
   # ------------------------------------------------------------ backward
-  def _vjp(self, uk, lam, beta) -> List[torch.Tensor]:
+  def _vjp(self, uk, lam, alpha, beta, out, x1=None, c1=0.0, x2=None,
+           c2=0.0) -> None:
+    """out = alpha*lam + c1*x1 + c2*x2 + beta*H^T J^T lam (interior)."""
     s = self.s
     nat.check(nat.load().swc_rk_stage_vjp(
         ctypes.byref(s.grid), ctypes.byref(s.scheme), s.bcs,
-        nat.ptr_array(uk), nat.ptr_array(lam), float(beta),
-        nat.ptr_array(self._vout), self._nu_bar.data_ptr(),
+        nat.ptr_array(uk), nat.ptr_array(lam), float(alpha), float(beta),
+        nat.ptr_array(x1) if x1 is not None else None, float(c1),
+        nat.ptr_array(x2) if x2 is not None else None, float(c2),
+        nat.ptr_array(out), self._nu_bar.data_ptr(),
         nat.ptr_array(self._scratch), nat.stream_ptr()), 'stage vjp')
-    return self._vout
 
-  def _interior_only(self, fields):
-    hw = self.s.hw
-    out = []
-    for f in fields:
-      g = torch.zeros_like(f)
-      g[hw:-hw, hw:-hw, hw:-hw] = f[hw:-hw, hw:-hw, hw:-hw]
-      out.append(g)
-    return out
+  def _reverse_step(self, stages, dt, g, gn, g2, g1) -> None:
+    """gn = cotangent of the step's input for the cotangent g of its
+    output."""
+    if self.order == 3:
+      u0, u1, u2 = stages
+      self._vjp(u2, g, 2.0 / 3.0, 2.0 / 3.0 * dt, g2)
+      self._vjp(u1, g2, 0.25, 0.25 * dt, g1)
+      self._vjp(u0, g1, 1.0, dt, gn, g, 1.0 / 3.0, g2, 0.75)
+    else:
+      u0, u1 = stages
+      self._vjp(u1, g, 0.5, 0.5 * dt, g1)
+      self._vjp(u0, g1, 1.0, dt, gn, g, 0.5)
 
   def backward(self, grad_out: Sequence[torch.Tensor]
                ) -> Tuple[List[torch.Tensor], float]:
@@ -117,36 +161,35 @@ class RunAdjoint:
     fields (interior cells; halos are ignored)."""
     if not self.checkpoints:
       raise RuntimeError('backward() needs a run() first.')
-    g = self._interior_only([x.to(self.s.dtype) for x in grad_out])
+    hw = self.s.hw
+    inner = (slice(hw, -hw),) * 3
+    g, gn, g2, g1 = self._g
+    for dst, src in zip(g, grad_out):
+      dst.zero_()
+      dst[inner] = src[inner].to(self.s.dtype)
     self._nu_bar.zero_()
     nsteps = len(self.dts)
-    for c in reversed(range(len(self.checkpoints))):
-      first = c * self.k
-      last = min(first + self.k, nsteps)
-      u = [f.clone() for f in self.checkpoints[c]]
-      stages = []
-      for i in range(first, last):
-        self._step(u, self.dts[i], keep=stages)
-      for i in reversed(range(first, last)):
-        dt = self.dts[i]
-        st = stages[i - first]
-        if self.order == 3:
-          u0, u1, u2 = st
-          v = self._vjp(u2, g, 2.0 / 3.0 * dt)
-          g2 = [2.0 / 3.0 * a + b for a, b in zip(g, v)]
-          v = self._vjp(u1, g2, 0.25 * dt)
-          g1 = [0.25 * a + b for a, b in zip(g2, v)]
-          v = self._vjp(u0, g1, dt)
-          g = [a / 3.0 + 0.75 * b + c + d for a, b, c, d in zip(g, g2, g1, v)]
-        else:
-          u0, u1 = st
-          v = self._vjp(u1, g, 0.5 * dt)
-          g1 = [0.5 * a + b for a, b in zip(g, v)]
-          v = self._vjp(u0, g1, dt)
-          g = [0.5 * a + b + c for a, b, c in zip(g, g1, v)]
-        g = self._interior_only(g)
-      del stages
-    return g, float(self._nu_bar.item())
+    if self.k == 0:
+      for i in reversed(range(nsteps)):
+        self._reverse_step(self._pool[i], self.dts[i], g, gn, g2, g1)
+        g, gn = gn, g
+    else:
+      self._reserve(min(self.k, nsteps))
+      for c in reversed(range(len(self.checkpoints))):
+        first = c * self.k
+        last = min(first + self.k, nsteps)
+        if self._u is None:
+          self._u = self.s.new_fields(zero=False)
+        u = self._u
+        for a, b in zip(u, self.checkpoints[c]):
+          a.copy_(b)
+        for i in range(first, last):
+          self._step(u, self.dts[i], self._pool[i - first])
+        for i in reversed(range(first, last)):
+          self._reverse_step(self._pool[i - first], self.dts[i], g, gn, g2,
+                             g1)
+          g, gn = gn, g
+    return [x.clone() for x in g], float(self._nu_bar.item())
 
 
 class _Run(torch.autograd.Function):
@@ -162,7 +205,7 @@ class _Run(torch.autograd.Function):
 
   @staticmethod
   def backward(ctx, *grads):
-    grads = [torch.zeros_like(ctx.runner.checkpoints[0][0]) if g is None else g
+    grads = [torch.zeros_like(ctx.runner._g[0][0]) if g is None else g
              for g in grads]
     gin, nub = ctx.runner.backward(grads)
     dtype, device = ctx.nu_meta

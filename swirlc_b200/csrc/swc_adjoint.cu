@@ -354,6 +354,10 @@ struct VjpArgs {
   double g[3];
   double* nu_bar;
   int seg;  // faces per thread along a line
+  // vout = alpha*lam + c1*x1 + c2*x2 + beta*H^T J^T lam on the interior.
+  double alpha, c1, c2;
+  const void* x1[5];
+  const void* x2[5];
 };
 
 template <typename T>
@@ -726,15 +730,47 @@ __global__ void vjp_halo_kernel(const VjpHalo a) {
       const T v = f[o];
       if (kind == SWC_BC_NONE) continue;
       f[o] = T(0);
-      if (kind == SWC_BC_PERIODIC) {
-        const long long src = side == 0 ? base + (long long)(l + n) * sd
-                                        : base + (long long)(a.h + l) * sd;
-        atomicAdd(f + src, v);
-      } else if (kind == SWC_BC_NEUMANN) {
-        const long long edge = side == 0 ? base + (long long)a.h * sd
-                                         : base + (long long)(n + a.h - 1) * sd;
-        atomicAdd(f + edge, v);
+      long long dst = -1;
+      if (kind == SWC_BC_PERIODIC)
+        dst = side == 0 ? base + (long long)(l + n) * sd
+                        : base + (long long)(a.h + l) * sd;
+      else if (kind == SWC_BC_NEUMANN)
+        dst = side == 0 ? base + (long long)a.h * sd
+                        : base + (long long)(n + a.h - 1) * sd;
+      if (dst < 0) continue;
+      // With n >= 2h the two sides' source cells are disjoint and each
+      // belongs to one thread: a plain update suffices.
+      if (n >= 2 * a.h) f[dst] += v;
+      else atomicAdd(f + dst, v);
+    }
+  }
+}
+
+// Interior: vout = alpha*lam + c1*x1 + c2*x2 + vout; halos: 0.
+template <typename T>
+__global__ void vjp_combine_kernel(const VjpArgs a) {
+  const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h, nza = a.nz + 2 * a.h;
+  const long long n = (long long)nxa * nya * nza;
+  const T al = T(a.alpha), c1 = T(a.c1), c2 = T(a.c2);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int ya = (int)(t % nya);
+    const int xa = (int)((t / nya) % nxa);
+    const int za = (int)(t / ((long long)nya * nxa));
+    const long long o = za * a.sz + xa * a.sx + ya;
+    const bool interior = xa >= a.h && xa < a.nx + a.h && ya >= a.h &&
+                          ya < a.ny + a.h && za >= a.h && za < a.nz + a.h;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      T* out = static_cast<T*>(a.vout[v]);
+      if (!interior) {
+        out[o] = T(0);
+        continue;
       }
+      T r = out[o] + al * static_cast<const T*>(a.lam[v])[o];
+      if (a.x1[v]) r += c1 * static_cast<const T*>(a.x1[v])[o];
+      if (a.x2[v]) r += c2 * static_cast<const T*>(a.x2[v])[o];
+      out[o] = r;
     }
   }
 }
@@ -787,6 +823,8 @@ int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
     vjp_halo_kernel<T><<<hb, 256, 0, s>>>(hh);
     note_launch();
   }
+  vjp_combine_kernel<T><<<pblocks, pt, 0, s>>>(a);
+  note_launch();
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? SWC_OK
                           : record_error(SWC_ERR_LAUNCH, "stage vjp: %s",
@@ -798,7 +836,9 @@ int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
 
 extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
                                 const SwcFieldBC* bcs, const void* const* uk,
-                                const void* const* lam, double beta,
+                                const void* const* lam, double alpha,
+                                double beta, const void* const* x1, double c1,
+                                const void* const* x2, double c2,
                                 void* const* vout, double* nu_bar,
                                 void* const* scratch, void* stream) {
   using namespace swc;
@@ -833,7 +873,15 @@ extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
     a.uk[v] = uk[v];
     a.lam[v] = lam[v];
     a.vout[v] = vout[v];
+    a.x1[v] = x1 ? x1[v] : nullptr;
+    a.x2[v] = x2 ? x2[v] : nullptr;
+    if (vout[v] == lam[v] || (x1 && x1[v] == vout[v]) ||
+        (x2 && x2[v] == vout[v]) || vout[v] == uk[v])
+      return record_error(SWC_ERR_ARG, "stage vjp: vout must not alias its inputs");
   }
+  a.alpha = alpha;
+  a.c1 = c1;
+  a.c2 = c2;
   for (int k = 0; k < 7; ++k) {
     a.prim[k] = scratch[k];
     a.pbar[k] = scratch[7 + k];

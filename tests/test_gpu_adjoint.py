@@ -178,6 +178,38 @@ def test_autograd_front_end_matches_reverse_sweep():
   assert float(nu.grad) == pytest.approx(nub2, rel=1e-12)
 
 
+def test_stored_stages_match_checkpointed_sweep():
+  """checkpoint_every=0 keeps every stage state instead of recomputing:
+  the same gradient (to summation order: the cotangents are accumulated
+  with atomic adds, so the last bits vary between runs)."""
+  from swirlc_b200 import adjoint, configs
+  cfg, state = configs.kelvin_helmholtz(n=12, nu=1e-2, dtype=np.float64)
+  _, s, f = _setup(cfg, state)
+  dts = [2e-3] * 5
+  res = []
+  for k in (0, 2):
+    run = adjoint.RunAdjoint(s, checkpoint_every=k)
+    o = run.run(f, dts)
+    res.append(run.backward(_loss_grad(s, o)))
+  for a, b in zip(res[0][0], res[1][0]):
+    torch.testing.assert_close(a, b, rtol=1e-12, atol=1e-14 * float(b.abs().max()))
+  assert res[0][1] == pytest.approx(res[1][1], rel=1e-12)
+
+
+def test_backward_twice_gives_the_same_gradient():
+  from swirlc_b200 import adjoint, configs
+  cfg, state = configs.kelvin_helmholtz(n=12, nu=1e-2, dtype=np.float64)
+  _, s, f = _setup(cfg, state)
+  run = adjoint.RunAdjoint(s, checkpoint_every=2, steps=5)
+  o = run.run(f, [2e-3] * 5)
+  g = _loss_grad(s, o)
+  a, na = run.backward(g)
+  b, nb = run.backward(g)
+  for x, y in zip(a, b):
+    torch.testing.assert_close(x, y, rtol=1e-12, atol=1e-14 * float(y.abs().max()))
+  assert na == pytest.approx(nb, rel=1e-12)
+
+
 def test_float32_adjoint_agrees_with_float64():
   from swirlc_b200 import adjoint, configs
   cfg, state = configs.kelvin_helmholtz(n=16, nu=1e-2, dtype=np.float64)
