@@ -6,7 +6,7 @@ unit cube of 256^3 interior cells, float32, WENO5-JS + HLLC + viscous
 Seeded synthetic initial condition (swirlc_b200.configs.kelvin_helmholtz).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload kh256|riemann_batch|adjoint]
+                  [--workload kh256|riemann_batch|adjoint|sod|bubble]
 
 Under torchrun each rank advances its own 256^3 domain (weak scaling,
 replicas; the halo exchange of a decomposed domain is a separate path).
@@ -638,6 +638,89 @@ def run_adjoint(args):
     print(json.dumps(line), flush=True)
 
 
+def _graph_steps(user_cfg, state, steps, warmup, dtype_name='f32'):
+  """Steps of the single-grid path replayed from a one-step CUDA graph:
+  (ms per step, the stepper). `warmup` steps run first on a throw-away copy
+  of the state, so that the timed run starts from the initial state."""
+  import torch
+  from swirlc_b200 import engine
+  from swirlc_b200.core import parameter
+  from swirlc_b200.physics import physics_models
+  dtype = torch.float32 if dtype_name == 'f32' else torch.float64
+  cfg = parameter.SwirlCParameters(user_cfg)
+  s = None
+
+  def stepper():
+    nonlocal s
+    f = [torch.tensor(state[k], dtype=dtype, device='cuda') for k in
+         ('rho', 'rho_u', 'rho_v', 'rho_w', 'rho_e')]
+    if s is None:
+      s = engine.Solver(cfg, physics_models.PhysicsModels(cfg), f[0].shape,
+                        dtype)
+    st = engine.Stepper(s, f, dt=cfg.dt, cfl=cfg.cfl, t_end=cfg.t_end,
+                        scheme=cfg.time_integration_scheme)
+    st.capture()
+    return st
+
+  warm = stepper()
+  warm.step(warmup)
+  del warm
+  st = stepper()
+  torch.cuda.synchronize()
+  e0, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(2))
+  e0.record()
+  st.step(steps)
+  e1.record()
+  torch.cuda.synchronize()
+  return e0.elapsed_time(e1) / steps, st
+
+
+def run_config_case(args):
+  """Config 1 (Sod 256x8x8 to t = 0.2) or config 3 (buoyant bubble
+  512x512x256, 50 steps): time per step under a CUDA graph and the float32
+  error against the same kernels in float64."""
+  import torch
+  from swirlc_b200 import accuracy, configs
+  if args.workload == 'sod':
+    user_cfg, state = configs.sod()
+    # Step count to t = 0.2 from a float64 run (its dt sequence is also the
+    # one the error report replays).
+    rep = accuracy.report('sod', user_cfg, state, 100000)
+    steps = rep['steps']
+    name = 'sod 256x8x8 fp32 WENO5+HLLC, CFL 0.5 to t = 0.2'
+  else:
+    user_cfg, state = configs.buoyant_bubble()
+    steps = 50
+    rep = accuracy.report('bubble', user_cfg, state, steps)
+    name = ('buoyant bubble 512x512x256 fp32 MUSCL(van Leer)+HLL, gravity, '
+            'Dirichlet/Neumann z walls, 50 steps, CFL 0.2')
+  sampler = ClockSampler(0)
+  sampler.start()
+  warmup = max(3, args.warmup)
+  ms, st = _graph_steps(user_cfg, state, steps, warmup)
+  clocks = sampler.stop()
+  s = st.s
+  cells = s.nx * s.ny * s.nz
+  line = {
+      'metric': f'{args.workload}: ms per SSP-RK3 step (CUDA graph) and '
+                'float32 error vs float64',
+      'value': ms, 'unit': 'ms/step', 'n_gpus': 1, 'steps': steps,
+      'warmup': warmup, 'ms_per_step': ms, 'higher_is_better': False,
+      'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+      'data': 'synthetic (configs.' + ('sod' if args.workload == 'sod'
+                                       else 'buoyant_bubble') + ')',
+      'config': {'workload': name, 'cells': cells,
+                 'l2': ('state resident in L2 (16k cells; time to solution)'
+                        if args.workload == 'sod' else
+                        'inputs larger than L2 (1.3 GB of fields)')},
+      'time_to_solution_ms': ms * steps,
+      'cell_updates_per_s': cells / (ms / 1e3),
+      'fp64_error': rep,
+      'clocks': clocks,
+  }
+  print(json.dumps(line), flush=True)
+
+
 def run_profile(args):
   """Eager RK3 steps of the workload, no timing: the command ncu captures."""
   import torch
@@ -767,7 +850,8 @@ def main():
                   help='adjoint workload: add the float64 16-direction '
                        'central-difference check at full size')
   ap.add_argument('--workload', default='kh256',
-                  choices=['kh256', 'riemann_batch', 'adjoint'],
+                  choices=['kh256', 'riemann_batch', 'adjoint', 'sod',
+                           'bubble'],
                   help='kh256: the headline 256^3 Kelvin-Helmholtz step; '
                        'riemann_batch: 64 batched Riemann problems')
   ap.add_argument('--profile-steps', type=int, default=0,
@@ -785,6 +869,8 @@ def main():
     run_batch(args)
   elif args.workload == 'adjoint':
     run_adjoint(args)
+  elif args.workload in ('sod', 'bubble'):
+    run_config_case(args)
   else:
     run_ours(args)
 

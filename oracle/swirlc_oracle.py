@@ -330,8 +330,18 @@ MUSCL_LIMITERS = ('van_leer', 'mc', 'minmod')
 
 def _limiter(r, kind):
   if kind == 'van_leer':
+    # From |r| >= 2^54 (2^25 in float32) 1 + |r| rounds to |r| and the
+    # formula gives exactly 2 (r > 0) or 0 (r < 0). Those values are taken
+    # directly there, which also covers ratios where r + |r| overflows or r
+    # is infinite (float64 keeps subnormals, so dm / dp overflows when dp is
+    # one), for which the formula gives inf or NaN. The CUDA limiter does
+    # the same.
     a = np.abs(r)
-    return (r + a) / (1.0 + a)
+    big = 2.0 ** 54 if r.dtype == np.float64 else 2.0 ** 25
+    with np.errstate(invalid='ignore', over='ignore'):
+      phi = (r + a) / (1.0 + a)
+    return np.where(a >= big, np.where(r > 0, 2.0, 0.0), phi).astype(
+        phi.dtype, copy=False)
   if kind == 'mc':
     return np.maximum(0.0, np.minimum(np.minimum(2.0 * r, 0.5 * (1.0 + r)), 2.0))
   if kind == 'minmod':

@@ -122,7 +122,11 @@ def buoyant_bubble(nx: int = 512, ny: int = 512, nz: int = 256, hw: int = 3,
   reference constant). +2 K Gaussian bubble of radius 0.2 lz centred at
   0.3 lz. Periodic x, y; z walls: rho_w Dirichlet 0, rho and rho_e
   Dirichlet to the hydrostatic profile, the rest Neumann 0. MUSCL (van Leer
-  limiter) + HLL, SSP-RK3."""
+  limiter) + HLL, SSP-RK3, CFL 0.2: with MUSCL (any limiter) the per-
+  direction CFL 0.5 of the other set-ups is unstable on this stratified
+  flow once dz is a few metres (|w| grows exponentially from round-off near
+  the bubble, in float32 and float64, with or without p_ref / rho_ref), while
+  0.2 stays bounded over the 50 steps."""
   lx = ly = lz * nx / nz
   cfg = _base_cfg(nx, ny, nz, lx, ly, lz, hw)
   t0, p0 = 300.0, 1.0e5
@@ -158,7 +162,7 @@ def buoyant_bubble(nx: int = 512, ny: int = 512, nz: int = 256, hw: int = 3,
       'numeric_flux_scheme': 'HLL', 'include_diffusion': False,
       'time_integration_scheme': 'rk3', 'g': {'x': 0.0, 'y': 0.0, 'z': -1.0},
       'source_functions': ['gravity'], 'bc': {'cell_averages': bc},
-      'cfl': 0.5, 'dt': 1e-3,
+      'cfl': 0.2, 'dt': 1e-3,
   })
   shape = (nz + 2 * hw, nx + 2 * hw, ny + 2 * hw)
   xh = _halo_coords(cfg['x'], hw).astype(np.float64)[np.newaxis, :, np.newaxis]

@@ -7,8 +7,12 @@ advances it num_cycles x num_steps steps in place with the fused stage
 kernels, one step captured in a CUDA graph and replayed. With cfg.cfl > 0
 the step size is the device-side CFL reduction, clamped to end at cfg.t_end
 when that is > 0; otherwise cfg.dt. `on_cycle(cycle, state, t)` is called
-after every cycle (e.g. to write the states out). Single replica; the
-domain-decomposed loop is swirlc_b200.parallel.
+after every cycle. With `dump_prefix` the configuration is saved as YAML
+and the conserved state (with the time) is written after every cycle at step
+start_step + (cycle + 1) * num_steps; with `load_prefix` the run restarts
+from the state written at cfg.start_step instead of calling the initializer
+(swirlc_b200.core.state_io gives the file layout). Single replica; the
+domain-decomposed loop is swirlc_b200.decomposition.
 """
 
 from typing import Callable, Dict, Optional
@@ -19,6 +23,7 @@ import torch
 from swirlc_b200 import engine
 from swirlc_b200.common import types
 from swirlc_b200.common import utils
+from swirlc_b200.core import state_io
 from swirlc_b200.physics import physics_models as physics_models_lib
 
 
@@ -54,16 +59,27 @@ def run(state: Dict[str, torch.Tensor], cfg, steps: int,
 
 
 def solver(customized_init_fn, cfg, on_cycle: Optional[Callable] = None,
-           dtype=torch.float32):
+           dtype=torch.float32, dump_prefix: Optional[str] = None,
+           load_prefix: Optional[str] = None):
   """driver.py:202-226: runs the simulation; returns the final state dict."""
   if cfg.cx * cfg.cy * cfg.cz != 1:
     raise NotImplementedError(
-        'Multi-replica runs go through swirlc_b200.parallel.')
-  init = customized_init_fn(0, (0, 0, 0), cfg)
+        'Multi-replica runs go through swirlc_b200.decomposition.')
   dev = torch.device('cuda', torch.cuda.current_device())
+  start = int(getattr(cfg, 'start_step', 0) or 0)
+  t0 = None
+  if load_prefix is not None:
+    init, t0 = state_io.load_state(load_prefix, types.BASE_CONSERVATIVE,
+                                   start, device=dev, dtype=dtype)
+  else:
+    init = customized_init_fn(0, (0, 0, 0), cfg)
   state = {k: utils.as_tensor3d(init[k]).to(device=dev, dtype=dtype)
            .contiguous() for k in types.BASE_CONSERVATIVE}
   stepper = run(state, cfg, 0)
+  if load_prefix is not None:
+    stepper.set_time(t0 if t0 is not None else start * float(cfg.dt), start)
+  if dump_prefix is not None:
+    cfg.save_to_file(dump_prefix)
   for cycle in range(cfg.num_cycles):
     if stepper.graph is None and cfg.num_steps > 1:
       stepper.step(1)
@@ -71,6 +87,11 @@ def solver(customized_init_fn, cfg, on_cycle: Optional[Callable] = None,
       stepper.step(cfg.num_steps - 1)
     else:
       stepper.step(cfg.num_steps)
+    if dump_prefix is not None:
+      torch.cuda.synchronize()
+      state_io.save_state(dump_prefix, state,
+                          start + (cycle + 1) * cfg.num_steps,
+                          names=types.BASE_CONSERVATIVE, t=stepper.time())
     if on_cycle is not None:
       torch.cuda.synchronize()
       on_cycle(cycle, state, stepper.time())

@@ -130,3 +130,74 @@ class SwirlCParameters:
       os.makedirs(output_dir, exist_ok=True)
     with open(f'{prefix}_swirl_c_cfg.yml', 'w') as f:
       yaml.dump(self._simulation_cfg, f, default_flow_style=False)
+
+  @classmethod
+  def load_from_file(cls, path: str) -> 'SwirlCParameters':
+    """Rebuilds the parameters from a file written by `save_to_file` (the
+    file name, or the prefix given to `save_to_file`)."""
+    if not path.endswith('.yml'):
+      path = f'{path}_swirl_c_cfg.yml'
+    with open(path) as f:
+      user_cfg = yaml.load(f, Loader=_CfgLoader)
+    if not isinstance(user_cfg, dict):
+      raise ValueError(f'{path} does not hold a configuration dictionary.')
+    return cls(user_cfg)
+
+
+class _CfgLoader(yaml.SafeLoader):
+  """Safe YAML plus the Python tags that `yaml.dump` writes for a
+  configuration: tuples, NumPy arrays, scalars and dtypes (in their pickle
+  form) and the BoundaryCondition enum (of either package). Any other Python
+  tag is an error: no other object is ever constructed."""
+
+
+_NP_RECONSTRUCT = ('numpy._core.multiarray._reconstruct',
+                   'numpy.core.multiarray._reconstruct')
+_NP_SCALAR = ('numpy._core.multiarray.scalar', 'numpy.core.multiarray.scalar')
+
+
+def _yaml_tuple(loader, node):
+  return tuple(loader.construct_sequence(node, deep=True))
+
+
+def _yaml_name(loader, suffix, node):
+  del loader, node
+  if suffix != 'numpy.ndarray':
+    raise yaml.constructor.ConstructorError(
+        None, None, f'python/name:{suffix} is not allowed in a configuration')
+  return np.ndarray
+
+
+def _np_dtype(args, state):
+  dt = np.dtype(args[0])
+  if state is not None and len(state) > 1 and state[1] in ('<', '>'):
+    dt = dt.newbyteorder(state[1])
+  return dt
+
+
+def _yaml_apply(loader, suffix, node):
+  if isinstance(node, yaml.SequenceNode):
+    args, state = loader.construct_sequence(node, deep=True), None
+  else:
+    m = loader.construct_mapping(node, deep=True)
+    args, state = m.get('args', []), m.get('state')
+  module, _, name = suffix.rpartition('.')
+  if name == 'BoundaryCondition' and module.endswith('bc_types'):
+    return bc_types.BoundaryCondition(args[0])
+  if suffix == 'numpy.dtype':
+    return _np_dtype(args, state)
+  if suffix in _NP_RECONSTRUCT and state is not None:
+    _, shape, dtype, fortran, raw = state
+    arr = np.frombuffer(raw, dtype=dtype)
+    return arr.reshape(shape, order='F' if fortran else 'C').copy()
+  if suffix in _NP_SCALAR:
+    return np.frombuffer(args[1], dtype=args[0])[0]
+  raise yaml.constructor.ConstructorError(
+      None, None, f'python/object/apply:{suffix} is not allowed in a '
+      'configuration', node.start_mark)
+
+
+_CfgLoader.add_constructor('tag:yaml.org,2002:python/tuple', _yaml_tuple)
+_CfgLoader.add_multi_constructor('tag:yaml.org,2002:python/name:', _yaml_name)
+_CfgLoader.add_multi_constructor('tag:yaml.org,2002:python/object/apply:',
+                                 _yaml_apply)

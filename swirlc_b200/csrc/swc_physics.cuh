@@ -186,8 +186,14 @@ __device__ __forceinline__ T muscl_slope(T vm1, T v0, T vp1, int limiter) {
   T r = dnn(dm, dp);
   T phi;
   if (limiter == 0) {  // van Leer
+    // From |r| >= 2^54 (2^25 in single precision) 1 + |r| rounds to |r| and
+    // the formula gives exactly 2 (r > 0) or 0 (r < 0); those values are
+    // taken directly there, which also covers ratios where r + |r|
+    // overflows or r is infinite (dp subnormal under dm: double precision
+    // keeps subnormals), for which the formula gives inf or NaN.
     T a = abs_(r);
-    phi = (r + a) / (T(1) + a);
+    const T big = sizeof(T) == 8 ? T(18014398509481984.0) : T(33554432.0);
+    phi = a >= big ? (r > T(0) ? T(2) : T(0)) : (r + a) / (T(1) + a);
   } else if (limiter == 1) {  // monotonized central
     phi = max_(T(0), min_(min_(T(2) * r, T(0.5) * (T(1) + r)), T(2)));
   } else {  // minmod

@@ -560,5 +560,10 @@ class Stepper:
   def time(self) -> float:
     return float(self.clock[0].item())
 
+  def set_time(self, t: float, steps: int = 0) -> None:
+    """Sets the clock's time and step count (a restarted run)."""
+    self.clock[0] = float(t)
+    self.clock[5:6].view(torch.int64).fill_(int(steps))
+
   def steps_done(self) -> int:
     return int(self.clock[5:6].view(torch.int64).item())

@@ -176,6 +176,36 @@ def test_reconstruction_matches_oracle(scheme, dtype):
                                  atol=tol, err_msg=f'{scheme} {dim}')
 
 
+@pytest.mark.parametrize('dtype', [torch.float32, torch.float64])
+def test_van_leer_extreme_ratios_stay_finite(dtype):
+  """Float64 keeps subnormals: beside a subnormal value dm / dp is +-inf or
+  a finite ratio whose r + |r| overflows (lines seen in the buoyant bubble
+  run in float64). From |r| >= 2^54 (2^25 in float32) van Leer's phi is
+  exactly 2 or 0, on the GPU and in the oracle alike, never inf or NaN."""
+  from swirlc_b200.numerics import interpolation
+  if dtype == torch.float64:
+    line = [5.67e-16, -1.41e-16, 7.9e-16, 5e-324, 0.0, 0.0, -5.70e-15,
+            5e-324, 0.0, -5e-324, 3e-15, 0.0, 5e-324, -5e-324, 1e-16, 2e-16]
+  else:
+    line = [0.5, -0.2, 5.0, 1.2e-38, 0.0, 0.0, -1.2e-38, 3.0, 0.0, 1.5e-38,
+            0.1, -4.0, -1.2e-38, 0.0, 0.2, 0.3]
+  npd = np.float64 if dtype == torch.float64 else np.float32
+  line = np.array(line, npd)
+  v = np.broadcast_to(line[None, None, :], (10, 10, line.size)).copy()
+  vt = torch.tensor(v, device='cuda')
+  got = interpolation.flux_limiter(vt, 'y',
+                                   interpolation.FluxLimiterType.VAN_LEER)
+  with np.errstate(over='ignore', divide='ignore'):
+    want = orc.muscl(v, 'y', 'van_leer')
+  # float32 runs flush-to-zero: values below its smallest normal may differ.
+  tol, atol = (1e-12, 1e-300) if dtype == torch.float64 else (2e-6, 1e-37)
+  sl = (slice(None), slice(None), slice(3, -3))
+  for g, w in zip(got, want):
+    g = g.cpu().numpy()[sl]
+    assert np.isfinite(g).all() and np.isfinite(w[sl]).all()
+    np.testing.assert_allclose(g, w[sl], rtol=tol, atol=atol)
+
+
 def test_exchange_halos_matches_boundary_test():
   """boundary_test.py:60-343 (single replica) through the CUDA halo fill."""
   from swirlc_b200.boundary import bc_types, boundary

@@ -35,6 +35,77 @@ def test_save_to_file(tmp_path):
   assert (tmp_path / 'run_swirl_c_cfg.yml').exists()
 
 
+def _same(a, b):
+  if isinstance(a, dict):
+    return a.keys() == b.keys() and all(_same(a[k], b[k]) for k in a)
+  if isinstance(a, (list, tuple)):
+    return (type(a) is type(b) and len(a) == len(b)
+            and all(_same(x, y) for x, y in zip(a, b)))
+  if isinstance(a, np.ndarray):
+    return (isinstance(b, np.ndarray) and a.dtype == b.dtype
+            and np.array_equal(a, b))
+  return type(a) is type(b) and a == b
+
+
+@pytest.mark.parametrize('case', ['default', 'bubble', 'kh'])
+def test_config_yaml_round_trip(tmp_path, case):
+  """save_to_file -> load_from_file rebuilds the same dictionary: NumPy
+  mesh arrays and scalars (dtype kept), BC enum tuples, Dirichlet planes."""
+  from swirlc_b200 import configs
+  user = {'default': lambda: None,
+          'bubble': lambda: configs.buoyant_bubble(nx=8, ny=8, nz=6)[0],
+          'kh': lambda: configs.kelvin_helmholtz(n=8)[0]}[case]()
+  cfg = parameter.SwirlCParameters(user)
+  prefix = str(tmp_path / 'sub' / case)
+  cfg.save_to_file(prefix)
+  back = parameter.SwirlCParameters.load_from_file(prefix)
+  assert _same(cfg._simulation_cfg, back._simulation_cfg)
+  back2 = parameter.SwirlCParameters.load_from_file(
+      prefix + '_swirl_c_cfg.yml')
+  assert _same(cfg._simulation_cfg, back2._simulation_cfg)
+
+
+def test_config_yaml_loader_rejects_other_python_objects(tmp_path):
+  import yaml
+  for text in ('x: !!python/object/apply:os.getcwd []\n',
+               'x: !!python/name:os.system \'\'\n',
+               'x: !!python/object:collections.OrderedDict {}\n'):
+    p = tmp_path / 'bad_swirl_c_cfg.yml'
+    p.write_text(text)
+    with pytest.raises(yaml.YAMLError):
+      parameter.SwirlCParameters.load_from_file(str(p))
+
+
+@pytest.mark.parametrize('dtype', [torch.float32, torch.float64])
+def test_state_files_round_trip(tmp_path, dtype):
+  from swirlc_b200.core import state_io
+  g = torch.Generator().manual_seed(0)
+  state = {k: torch.rand((7, 9, 11), generator=g, dtype=dtype)
+           for k in types.BASE_CONSERVATIVE}
+  prefix = str(tmp_path / 'a' / 'run')
+  state_io.save_state(prefix, state, 40, coordinate=(1, 0, 2), t=0.125)
+  assert (tmp_path / 'a' / 'run-field-rho_e-xyz-1-0-2-step-40.npy').exists()
+  back, t = state_io.load_state(prefix, types.BASE_CONSERVATIVE, 40,
+                                coordinate=(1, 0, 2))
+  assert t == 0.125
+  for k in state:
+    assert back[k].dtype == dtype and torch.equal(back[k], state[k])
+  back64, _ = state_io.load_state(prefix, ['rho'], 40, (1, 0, 2),
+                                  dtype=torch.float64)
+  assert back64['rho'].dtype == torch.float64
+  state_io.save_state(prefix, {'rho': state['rho']}, 41)
+  assert state_io.load_state(prefix, ['rho'], 41)[1] is None
+  with pytest.raises(FileNotFoundError):
+    state_io.load_state(prefix, ['rho'], 39, (1, 0, 2))
+  with pytest.raises(KeyError):
+    state_io.save_state(prefix, state, 42, names=['rho_y'])
+  state_io.save_state(prefix, {'rho': state['rho'],
+                               'rho_u': state['rho_u'][:, :, :5]}, 43)
+  with pytest.raises(ValueError):
+    state_io.load_state(prefix, ['rho', 'rho_u'], 43)
+  assert not list((tmp_path / 'a').glob('*.tmp*'))
+
+
 def test_physics_models_selection_errors():
   with pytest.raises(NotImplementedError):
     physics_models.PhysicsModels(
