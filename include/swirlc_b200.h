@@ -264,9 +264,11 @@ int swc_batch_step(const SwcScheme* scheme, int32_t order, int32_t nmembers,
  * read). A stage out = A*u0 + B*(uk + dt*L(uk)) (rk3.py:87-120) has the uk
  * cotangent B*lam + B*dt*H^T J^T lam (alpha = B, beta = B*dt) and the u0
  * cotangent A*lam, which x1 / x2 let the caller fold in. vout must not alias
- * uk, lam, x1 or x2. `scratch` is 14 caller buffers of the shape of uk. The
- * reference differentiates this path with TF's GradientTape; this is its
- * discrete adjoint. */
+ * uk, lam, x1 or x2. `scratch` is SWC_VJP_SCRATCH caller buffers of the
+ * shape of uk (primitives and their cotangents, and copies transposed to
+ * [z][y][x] for the y faces). The reference differentiates this path with
+ * TF's GradientTape; this is its discrete adjoint. */
+#define SWC_VJP_SCRATCH 33
 int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* scheme,
                      const SwcFieldBC* bcs, const void* const* uk,
                      const void* const* lam, double alpha, double beta,

@@ -55,7 +55,8 @@ class RunAdjoint:
     self.checkpoints: List[List[torch.Tensor]] = []
     self.dts: List[float] = []
     self._scratch = [torch.empty(solver.shape, dtype=solver.dtype,
-                                 device=solver.device) for _ in range(14)]
+                                 device=solver.device)
+                     for _ in range(nat.SWC_VJP_SCRATCH)]
     self._g = [solver.new_fields(zero=True) for _ in range(4)]
     self._nu_bar = torch.zeros(1, dtype=torch.float64, device=solver.device)
     self._pool: List = []  # per-step stage buffers, reused

@@ -29,10 +29,13 @@ namespace {
 // Reverse of the pieces of one face flux.
 // ---------------------------------------------------------------------------
 
-// WENO5 face value from v[0..4] (right face of v[2] when RIGHT, left face of
-// v[2] otherwise): vb[k] += dout/dv[k] * ob.
-template <typename T, bool RIGHT>
-__device__ __forceinline__ void weno5_vjp(const T* v, T ob, T* vb) {
+// Reverse of reconstruct_cell<0> (swc_physics.cuh): both WENO5 face values
+// of the cell v[2] from v[0..4] = v[c-2 .. c+2], which share the smoothness
+// indicators. vb[k] += d right/dv[k] * rb + d left/dv[k] * lb.
+template <typename T>
+__device__ __forceinline__ void weno5_cell_vjp(const T* v, T rb, T lb, T* vb) {
+  // Per stencil r: a_r = sum A[r][k] v[k], b_r = sum Bc[r][k] v[k],
+  // beta_r = 13/12 a_r^2 + 1/4 b_r^2 + eps, candidate q_r = sum Q[r][k] v[k].
   constexpr double A[3][5] = {{0, 0, 1, -2, 1}, {0, 1, -2, 1, 0}, {1, -2, 1, 0, 0}};
   constexpr double Bc[3][5] = {{0, 0, 3, -4, 1}, {0, 1, 0, -1, 0}, {1, -4, 3, 0, 0}};
   constexpr double QR[3][5] = {{0, 0, 1.0 / 3, 5.0 / 6, -1.0 / 6},
@@ -43,34 +46,52 @@ __device__ __forceinline__ void weno5_vjp(const T* v, T ob, T* vb) {
                                {-1.0 / 6, 5.0 / 6, 1.0 / 3, 0, 0}};
   constexpr double DR[3] = {0.3, 0.6, 0.1}, DL[3] = {0.1, 0.6, 0.3};
   const T c1312 = T(13.0 / 12.0), eps = T(1e-6);
-  T av[3], bv[3], be[3], al[3], q[3];
+  T av[3], bv[3], ib[3], iq[3], qr[3], ql[3];
+  T sr = T(0), sl = T(0), nr = T(0), nl = T(0);
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
-    T sa = T(0), sb = T(0), sq = T(0);
+    T sa = T(0), sb = T(0), sqr = T(0), sql = T(0);
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
-      sa += T(A[r][k]) * v[k];
-      sb += T(Bc[r][k]) * v[k];
-      sq += T(RIGHT ? QR[r][k] : QL[r][k]) * v[k];
+      if (A[r][k] != 0) sa += T(A[r][k]) * v[k];
+      if (Bc[r][k] != 0) sb += T(Bc[r][k]) * v[k];
+      if (QR[r][k] != 0) sqr += T(QR[r][k]) * v[k];
+      if (QL[r][k] != 0) sql += T(QL[r][k]) * v[k];
     }
     av[r] = sa;
     bv[r] = sb;
-    q[r] = sq;
-    be[r] = c1312 * sa * sa + T(0.25) * sb * sb + eps;
-    al[r] = T(RIGHT ? DR[r] : DL[r]) / (be[r] * be[r]);
+    qr[r] = sqr;
+    ql[r] = sql;
+    const T be = c1312 * sa * sa + T(0.25) * sb * sb + eps;
+    ib[r] = rcp_(be);           // 1 / beta_r
+    iq[r] = ib[r] * ib[r];      // 1 / beta_r^2
+    sr += T(DR[r]) * iq[r];
+    sl += T(DL[r]) * iq[r];
+    nr += T(DR[r]) * iq[r] * sqr;
+    nl += T(DL[r]) * iq[r] * sql;
   }
-  const T S = al[0] + al[1] + al[2];
-  const T out = (al[0] * q[0] + al[1] * q[1] + al[2] * q[2]) / S;
+  const T isr = rcp_(sr), isl = rcp_(sl);
+  const T outr = nr * isr, outl = nl * isl;
+  const T gr = rb * isr, gl = lb * isl;
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
-    const T qb = ob * al[r] / S;
-    const T ab = ob * (q[r] - out) / S;
-    const T bb = T(-2) * ab * al[r] / be[r];
+    // alpha_r = D_r / beta_r^2; out = sum alpha q / sum alpha.
+    const T qbr = gr * T(DR[r]) * iq[r];
+    const T qbl = gl * T(DL[r]) * iq[r];
+    const T ibq = gr * T(DR[r]) * (qr[r] - outr) + gl * T(DL[r]) * (ql[r] - outl);
+    // d(1/beta^2)/d beta = -2 / beta^3
+    const T bb = T(-2) * ibq * iq[r] * ib[r];
+    const T ca = bb * T(2) * c1312 * av[r];
+    const T cb = bb * T(0.5) * bv[r];
 #pragma unroll
-    for (int k = 0; k < 5; ++k)
-      vb[k] += qb * T(RIGHT ? QR[r][k] : QL[r][k]) +
-               bb * (T(2) * c1312 * av[r] * T(A[r][k]) +
-                     T(0.5) * bv[r] * T(Bc[r][k]));
+    for (int k = 0; k < 5; ++k) {
+      T t = T(0);
+      if (QR[r][k] != 0) t += qbr * T(QR[r][k]);
+      if (QL[r][k] != 0) t += qbl * T(QL[r][k]);
+      if (A[r][k] != 0) t += ca * T(A[r][k]);
+      if (Bc[r][k] != 0) t += cb * T(Bc[r][k]);
+      vb[k] += t;
+    }
   }
 }
 
@@ -343,7 +364,14 @@ struct VjpArgs {
   const void* uk[5];
   const void* lam[5];
   void* prim[7];  // rho, u, v, w, e, p, h of uk, every cell
-  void* pbar[7];  // primitive cotangents, every cell
+  void* pbar[7];  // primitive cotangents of the x and z faces, every cell
+  // Copies in the layout [z][y][x] (x contiguous) for the y faces, whose
+  // lines run along the contiguous axis of the reference layout: the
+  // primitives, lam, and the y faces' primitive cotangents.
+  void* primT[7];
+  void* lamT[5];
+  void* pbarT[7];
+  long long tsy, tsz;  // y and z strides of the transposed layout
   void* vout[5];  // conserved cotangents, every cell
   const void* pe[3];
   int has_pe;
@@ -369,48 +397,105 @@ __device__ __forceinline__ T pe_of(const VjpArgs& a, int xa, int ya, int za) {
   return (-(px ? px[xa] : T(0)) - (py ? py[ya] : T(0))) - (pz ? pz[za] : T(0));
 }
 
-// Primitives of every cell (halos included).
+// Tiles of the prim and cell kernels: a (32, 8) block covers 32 x 32 (y, x)
+// cells of one z plane, 4 per thread; the transposed copies go through a
+// shared-memory tile so that both layouts are read and written coalesced.
+constexpr int TT = 32;
+
+// Primitives of every cell (halos included), in both layouts, with their
+// cotangent buffers cleared, and lam transposed.
 template <typename T>
-__global__ void vjp_prim_kernel(const VjpArgs a) {
-  const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h, nza = a.nz + 2 * a.h;
-  const long long n = (long long)nxa * nya * nza;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int ya = (int)(t % nya);
-    const int xa = (int)((t / nya) % nxa);
-    const int za = (int)(t / ((long long)nya * nxa));
+__global__ void __launch_bounds__(256) vjp_prim_kernel(const VjpArgs a) {
+  __shared__ T tile[TT][TT + 1];
+  const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h;
+  const int za = blockIdx.z;
+  const int y0 = blockIdx.x * TT, x0 = blockIdx.y * TT;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  T pr[4][7];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+#pragma unroll
+    for (int v = 0; v < 7; ++v) pr[k][v] = T(0);
+    const int xa = x0 + ty + 8 * k, ya = y0 + tx;
+    if (xa >= nxa || ya >= nya) continue;
     const long long o = za * a.sz + xa * a.sx + ya;
     T c[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) c[v] = static_cast<const T*>(a.uk[v])[o];
-    T u, v, w, e, p, hh;
-    cons_to_prim(c[0], c[1], c[2], c[3], c[4], pe_of<T>(a, xa, ya, za), u, v,
-                 w, e, p, hh);
-    const T pr[7] = {c[0], u, v, w, e, p, hh};
+    T u, vv, w, e, p, hh;
+    cons_to_prim(c[0], c[1], c[2], c[3], c[4], pe_of<T>(a, xa, ya, za), u,
+                 vv, w, e, p, hh);
+    pr[k][0] = c[0]; pr[k][1] = u; pr[k][2] = vv; pr[k][3] = w;
+    pr[k][4] = e; pr[k][5] = p; pr[k][6] = hh;
 #pragma unroll
-    for (int k = 0; k < 7; ++k) static_cast<T*>(a.prim[k])[o] = pr[k];
+    for (int v = 0; v < 7; ++v) {
+      static_cast<T*>(a.prim[v])[o] = pr[k][v];
+      static_cast<T*>(a.pbar[v])[o] = T(0);
+    }
+  }
+  // tile[x - x0][y - y0]; the transposed write reads it along x.
+  for (int v = 0; v < 12; ++v) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (v < 7) {
+        tile[ty + 8 * k][tx] = pr[k][v];
+      } else {
+        const int xa = x0 + ty + 8 * k, ya = y0 + tx;
+        tile[ty + 8 * k][tx] =
+            (xa < nxa && ya < nya)
+                ? static_cast<const T*>(a.lam[v - 7])[za * a.sz + xa * a.sx + ya]
+                : T(0);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int yl = ty + 8 * k;
+      const int xa = x0 + tx, ya = y0 + yl;
+      if (xa >= nxa || ya >= nya) continue;
+      const long long ot = za * a.tsz + ya * a.tsy + xa;
+      if (v < 7) {
+        static_cast<T*>(a.primT[v])[ot] = tile[tx][yl];
+        static_cast<T*>(a.pbarT[v])[ot] = T(0);
+      } else {
+        static_cast<T*>(a.lamT[v - 7])[ot] = tile[tx][yl];
+      }
+    }
+    __syncthreads();
   }
 }
 
 // Face VJPs along dim D. Thread = `seg` consecutive faces of one line along
 // D; a register window holds the 6-cell stencil primitives and their
 // cotangents, and a cell's cotangents are added to pbar once, when the
-// window leaves it.
+// window leaves it. Neighbouring threads take neighbouring lines along the
+// contiguous axis: y for the x and z faces in the reference layout, x for
+// the y faces, which run on the transposed copies.
+// Minimum resident blocks of the face kernel (its register budget).
+#ifndef SWC_VJP_FACE_MINB
+#define SWC_VJP_FACE_MINB 1
+#endif
+
 template <typename T, int D>
-__global__ void __launch_bounds__(128) vjp_face_kernel(const VjpArgs a) {
+__global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
+    vjp_face_kernel(const VjpArgs a) {
   const int h = a.h;
   const int n = D == 0 ? a.nx : (D == 1 ? a.ny : a.nz);
   // Transverse axes (t1, t2) of the rotated frame: x:(y,z) y:(x,z) z:(x,y).
   const int n1 = D == 0 ? a.ny : a.nx;
   const int n2 = D == 2 ? a.ny : a.nz;
-  const long long st = D == 0 ? a.sx : (D == 1 ? 1 : a.sz);
-  const long long s1 = D == 0 ? 1 : a.sx;
-  const long long s2 = D == 2 ? 1 : a.sz;
+  const long long st = D == 0 ? a.sx : (D == 1 ? a.tsy : a.sz);
+  const long long s1 = D == 2 ? a.sx : 1;
+  const long long s2 = D == 0 ? a.sz : (D == 1 ? a.tsz : 1);
+  void* const* PBAR = D == 1 ? a.pbarT : a.pbar;
+  const void* const* LAM = D == 1 ? const_cast<const void* const*>(a.lamT)
+                                  : a.lam;
   const T hd = T(D == 0 ? a.dx : (D == 1 ? a.dy : a.dz));
   const T h1 = T(D == 0 ? a.dy : a.dx);
   const T h2 = T(D == 2 ? a.dy : a.dz);
   const int nseg = (n + 1 + a.seg - 1) / a.seg;
-  // Thread index: the coordinate along y varies fastest (coalesced loads).
+  // Thread index: the transverse coordinate along the contiguous axis
+  // varies fastest (coalesced loads and atomics).
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long lines = (long long)n1 * n2;
   // Threads past the last line take no faces but join the nu reduction.
@@ -421,7 +506,7 @@ __global__ void __launch_bounds__(128) vjp_face_kernel(const VjpArgs a) {
     if (D == 2) {  // (t1, t2) = (x, y): y fastest
       c2 = (int)(r % n2); r /= n2;
       c1 = (int)(r % n1); r /= n1;
-    } else {  // t1 is y for D = 0; for D = 1, t1 = x
+    } else {  // t1: y for D = 0; x (contiguous when transposed) for D = 1
       c1 = (int)(r % n1); r /= n1;
       c2 = (int)(r % n2); r /= n2;
     }
@@ -433,7 +518,8 @@ __global__ void __launch_bounds__(128) vjp_face_kernel(const VjpArgs a) {
   const int vel[3] = {1 + D, D == 0 ? 2 : 1, D == 2 ? 2 : 3};
   const T* P[7];
 #pragma unroll
-  for (int k = 0; k < 7; ++k) P[k] = static_cast<const T*>(a.prim[k]);
+  for (int k = 0; k < 7; ++k)
+    P[k] = static_cast<const T*>(D == 1 ? a.primT[k] : a.prim[k]);
   // Rotated primitive of cell j (normal index with halo = j + h).
   auto load = [&](int j, T* q) {
     const long long o = base + (long long)(j + h) * st;
@@ -453,37 +539,79 @@ __global__ void __launch_bounds__(128) vjp_face_kernel(const VjpArgs a) {
     }
     const long long o = base + (long long)(j + h) * st;
 #pragma unroll
-    for (int v = 0; v < 5; ++v) lv[v] = static_cast<const T*>(a.lam[v])[o];
+    for (int v = 0; v < 5; ++v) lv[v] = static_cast<const T*>(LAM[v])[o];
   };
   auto flush = [&](int j, const T* b) {
     const long long o = base + (long long)(j + h) * st;
-    atomicAdd(static_cast<T*>(a.pbar[0]) + o, b[0]);
-    atomicAdd(static_cast<T*>(a.pbar[vel[0]]) + o, b[1]);
-    atomicAdd(static_cast<T*>(a.pbar[vel[1]]) + o, b[2]);
-    atomicAdd(static_cast<T*>(a.pbar[vel[2]]) + o, b[3]);
-    atomicAdd(static_cast<T*>(a.pbar[4]) + o, b[4]);
-    atomicAdd(static_cast<T*>(a.pbar[5]) + o, b[5]);
-    atomicAdd(static_cast<T*>(a.pbar[6]) + o, b[6]);
+    atomicAdd(static_cast<T*>(PBAR[0]) + o, b[0]);
+    atomicAdd(static_cast<T*>(PBAR[vel[0]]) + o, b[1]);
+    atomicAdd(static_cast<T*>(PBAR[vel[1]]) + o, b[2]);
+    atomicAdd(static_cast<T*>(PBAR[vel[2]]) + o, b[3]);
+    atomicAdd(static_cast<T*>(PBAR[4]) + o, b[4]);
+    atomicAdd(static_cast<T*>(PBAR[5]) + o, b[5]);
+    atomicAdd(static_cast<T*>(PBAR[6]) + o, b[6]);
   };
-  // Window: cells i-3 .. i+2 for face i (face i-1/2 between i-1 and i).
-  T sw[6][7], ab[6][7];
+  // Window at face i (between cells i-1 and i): primitives sw[k] of cells
+  // i-3+k (k = 0..5) and cotangents ab[k] of cells i-3+k (k = 0..4). Step i
+  // reconstructs cell i (its left value is face i's right state; its right
+  // value is carried to face i+1), reverses face i's flux, and then reverses
+  // cell i-1's reconstruction with the cotangents of both of its face values
+  // (face i-1's, carried, and face i's). A cell whose two faces belong to two
+  // threads is reversed by both, each with its own face's cotangent (the
+  // reverse is linear in them). Cells leave the window complete.
+  T sw[6][7], ab[5][7];
 #pragma unroll
   for (int k = 0; k < 5; ++k) {
 #pragma unroll
     for (int v = 0; v < 7; ++v) ab[k][v] = T(0);
   }
-#pragma unroll
-  for (int v = 0; v < 7; ++v) ab[5][v] = T(0);
+  T qn[7], cl[7];  // right value of cell i-1; cotangent of its left value
   T la[5], lb[5];
+#pragma unroll
+  for (int v = 0; v < 7; ++v) {
+    qn[v] = T(0);
+    cl[v] = T(0);
+  }
   if (active) {
 #pragma unroll
-  for (int k = 0; k < 5; ++k) load(i0 - 3 + k, sw[k]);
+    for (int k = 0; k < 5; ++k) load(i0 - 3 + k, sw[k]);
+#pragma unroll
+    for (int v = 0; v < 7; ++v) {
+      const T s5[5] = {sw[0][v], sw[1][v], sw[2][v], sw[3][v], sw[4][v]};
+      T lv, rv;
+      reconstruct_cell<0>(s5, 0, lv, rv);
+      qn[v] = rv;
+    }
   }
   lam_at(active ? i0 - 1 : -1, la);
   const T scale = T(a.beta) / hd;
   const T nu = T(a.nu), inv_pr = T(1.0 / a.pr);
-  const T gam = K<T>::gamma();
-  (void)gam;
+  const T i2t1 = T(1) / (T(2) * h1), i2t2 = T(1) / (T(2) * h2);
+  T* PB1 = static_cast<T*>(PBAR[vel[1]]);
+  T* PB0 = static_cast<T*>(PBAR[vel[0]]);
+  T* PB2 = static_cast<T*>(PBAR[vel[2]]);
+  // Viscous: tangential central differences of cell o (g11, g10, g22, g20:
+  // velocity t1 and the normal velocity along t1, velocity t2 and the normal
+  // velocity along t2), and the reverse onto the four neighbours.
+  auto tang = [&](long long o, T* g4) {
+    g4[0] = (P[vel[1]][o + s1] - P[vel[1]][o - s1]) * i2t1;
+    g4[1] = (P[vel[0]][o + s1] - P[vel[0]][o - s1]) * i2t1;
+    g4[2] = (P[vel[2]][o + s2] - P[vel[2]][o - s2]) * i2t2;
+    g4[3] = (P[vel[0]][o + s2] - P[vel[0]][o - s2]) * i2t2;
+  };
+  auto tang_flush = [&](long long o, const T* gb) {
+    atomicAdd(PB1 + o + s1, gb[0] * i2t1);
+    atomicAdd(PB1 + o - s1, -gb[0] * i2t1);
+    atomicAdd(PB0 + o + s1, gb[1] * i2t1);
+    atomicAdd(PB0 + o - s1, -gb[1] * i2t1);
+    atomicAdd(PB2 + o + s2, gb[2] * i2t2);
+    atomicAdd(PB2 + o - s2, -gb[2] * i2t2);
+    atomicAdd(PB0 + o + s2, gb[3] * i2t2);
+    atomicAdd(PB0 + o - s2, -gb[3] * i2t2);
+  };
+  // Tangential differences of cell i-1 and their cotangent so far.
+  T g4a[4] = {T(0), T(0), T(0), T(0)}, gba[4] = {T(0), T(0), T(0), T(0)};
+  if (a.visc && active) tang(base + (long long)(i0 - 1 + h) * st, g4a);
   T nub = T(0);
   for (int i = i0; i < i1; ++i) {
     load(i + 2, sw[5]);
@@ -498,23 +626,18 @@ __global__ void __launch_bounds__(128) vjp_face_kernel(const VjpArgs a) {
     fr[2] = fb[1 + (D == 0 ? 1 : 0)];
     fr[3] = fb[1 + (D == 2 ? 1 : 2)];
     fr[4] = fb[4];
-    // Forward face states.
-    Prim<T> ql, qr;
-    {
-      T s[6];
-      T neg[7], pos[7];
+    // Forward: cell i from cells i-2 .. i+2; face i's states.
+    T lv[7], rn[7];
 #pragma unroll
-      for (int v = 0; v < 7; ++v) {
-#pragma unroll
-        for (int k = 0; k < 6; ++k) s[k] = sw[k][v];
-        neg[v] = weno5_right(s[0], s[1], s[2], s[3], s[4]);
-        pos[v] = weno5_left(s[1], s[2], s[3], s[4], s[5]);
-      }
-      ql.r = neg[0]; ql.u[0] = neg[1]; ql.u[1] = neg[2]; ql.u[2] = neg[3];
-      ql.e = neg[4]; ql.p = neg[5]; ql.h = neg[6];
-      qr.r = pos[0]; qr.u[0] = pos[1]; qr.u[1] = pos[2]; qr.u[2] = pos[3];
-      qr.e = pos[4]; qr.p = pos[5]; qr.h = pos[6];
+    for (int v = 0; v < 7; ++v) {
+      const T s5[5] = {sw[1][v], sw[2][v], sw[3][v], sw[4][v], sw[5][v]};
+      reconstruct_cell<0>(s5, 0, lv[v], rn[v]);
     }
+    Prim<T> ql, qr;
+    ql.r = qn[0]; ql.u[0] = qn[1]; ql.u[1] = qn[2]; ql.u[2] = qn[3];
+    ql.e = qn[4]; ql.p = qn[5]; ql.h = qn[6];
+    qr.r = lv[0]; qr.u[0] = lv[1]; qr.u[1] = lv[2]; qr.u[2] = lv[3];
+    qr.e = lv[4]; qr.p = lv[5]; qr.h = lv[6];
     int xa, ya, za;  // face cell b = i (pe at the face index)
     {
       const int jb = i + h;
@@ -527,44 +650,18 @@ __global__ void __launch_bounds__(128) vjp_face_kernel(const VjpArgs a) {
     lbar.zero();
     rbar.zero();
     hllc_vjp<T>(ql, qr, pe, fr, lbar, rbar);
-    {
-      const T nb[7] = {lbar.r, lbar.u[0], lbar.u[1], lbar.u[2], lbar.e, lbar.p, lbar.h};
-      const T pb[7] = {rbar.r, rbar.u[0], rbar.u[1], rbar.u[2], rbar.e, rbar.p, rbar.h};
-#pragma unroll
-      for (int v = 0; v < 7; ++v) {
-        T s[6], sb[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-#pragma unroll
-        for (int k = 0; k < 6; ++k) s[k] = sw[k][v];
-        weno5_vjp<T, true>(s, nb[v], sb);
-        weno5_vjp<T, false>(s + 1, pb[v], sb + 1);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) ab[k][v] += sb[k];
-      }
-    }
     if (a.visc) {
-      // Cells a = i-1 (window 2) and b = i (window 3) and the tangential
-      // neighbours of both for the cross derivatives.
+      // Cells a = i-1 (window 2) and b = i (window 3).
       const T* ca = sw[2];
       const T* cb = sw[3];
-      const long long oa = base + (long long)(i - 1 + h) * st;
-      const long long ob = oa + st;
-      T ga4[4], gb4[4];
-      const T i2t1 = T(1) / (T(2) * h1), i2t2 = T(1) / (T(2) * h2);
-      // g11: t1 derivative of velocity t1; g10: of the normal velocity;
-      // g22 / g20 likewise along t2.
-      ga4[0] = (P[vel[1]][oa + s1] - P[vel[1]][oa - s1]) * i2t1;
-      ga4[1] = (P[vel[0]][oa + s1] - P[vel[0]][oa - s1]) * i2t1;
-      ga4[2] = (P[vel[2]][oa + s2] - P[vel[2]][oa - s2]) * i2t2;
-      ga4[3] = (P[vel[0]][oa + s2] - P[vel[0]][oa - s2]) * i2t2;
-      gb4[0] = (P[vel[1]][ob + s1] - P[vel[1]][ob - s1]) * i2t1;
-      gb4[1] = (P[vel[0]][ob + s1] - P[vel[0]][ob - s1]) * i2t1;
-      gb4[2] = (P[vel[2]][ob + s2] - P[vel[2]][ob - s2]) * i2t2;
-      gb4[3] = (P[vel[0]][ob + s2] - P[vel[0]][ob - s2]) * i2t2;
+      const long long ob = base + (long long)(i + h) * st;
+      T g4b[4];
+      tang(ob, g4b);
       T rab = T(0), rbb = T(0), pab = T(0), pbb = T(0);
       T uab[3] = {T(0), T(0), T(0)}, ubb[3] = {T(0), T(0), T(0)};
       T gab[4] = {T(0), T(0), T(0), T(0)}, gbb[4] = {T(0), T(0), T(0), T(0)};
       const T ua[3] = {ca[1], ca[2], ca[3]}, ub[3] = {cb[1], cb[2], cb[3]};
-      nub += viscous_vjp<T>(ca[0], cb[0], ua, ub, ca[5], cb[5], ga4, gb4, hd,
+      nub += viscous_vjp<T>(ca[0], cb[0], ua, ub, ca[5], cb[5], g4a, g4b, hd,
                             nu, inv_pr, fr, rab, rbb, uab, ubb, pab, pbb, gab,
                             gbb);
       ab[2][0] += rab;
@@ -576,46 +673,65 @@ __global__ void __launch_bounds__(128) vjp_face_kernel(const VjpArgs a) {
         ab[2][1 + c] += uab[c];
         ab[3][1 + c] += ubb[c];
       }
-      // Tangential neighbours: cotangents of the central differences.
-      T* PB1 = static_cast<T*>(a.pbar[vel[1]]);
-      T* PB0 = static_cast<T*>(a.pbar[vel[0]]);
-      T* PB2 = static_cast<T*>(a.pbar[vel[2]]);
-      atomicAdd(PB1 + oa + s1, gab[0] * i2t1);
-      atomicAdd(PB1 + oa - s1, -gab[0] * i2t1);
-      atomicAdd(PB0 + oa + s1, gab[1] * i2t1);
-      atomicAdd(PB0 + oa - s1, -gab[1] * i2t1);
-      atomicAdd(PB2 + oa + s2, gab[2] * i2t2);
-      atomicAdd(PB2 + oa - s2, -gab[2] * i2t2);
-      atomicAdd(PB0 + oa + s2, gab[3] * i2t2);
-      atomicAdd(PB0 + oa - s2, -gab[3] * i2t2);
-      atomicAdd(PB1 + ob + s1, gbb[0] * i2t1);
-      atomicAdd(PB1 + ob - s1, -gbb[0] * i2t1);
-      atomicAdd(PB0 + ob + s1, gbb[1] * i2t1);
-      atomicAdd(PB0 + ob - s1, -gbb[1] * i2t1);
-      atomicAdd(PB2 + ob + s2, gbb[2] * i2t2);
-      atomicAdd(PB2 + ob - s2, -gbb[2] * i2t2);
-      atomicAdd(PB0 + ob + s2, gbb[3] * i2t2);
-      atomicAdd(PB0 + ob - s2, -gbb[3] * i2t2);
+      // Cell i-1's tangential cotangent is complete (faces i-1 and i).
+#pragma unroll
+      for (int c = 0; c < 4; ++c) gba[c] += gab[c];
+      tang_flush(ob - st, gba);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        gba[c] = gbb[c];
+        g4a[c] = g4b[c];
+      }
     }
-    // Cell i-3 is complete for this thread: flush it and slide.
+    // Reverse of cell i-1's reconstruction (cells i-3 .. i+1).
+    {
+      const T cr[7] = {lbar.r, lbar.u[0], lbar.u[1], lbar.u[2], lbar.e, lbar.p, lbar.h};
+#pragma unroll
+      for (int v = 0; v < 7; ++v) {
+        const T s5[5] = {sw[0][v], sw[1][v], sw[2][v], sw[3][v], sw[4][v]};
+        T sb[5] = {T(0), T(0), T(0), T(0), T(0)};
+        weno5_cell_vjp<T>(s5, cr[v], cl[v], sb);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) ab[k][v] += sb[k];
+      }
+      const T cn[7] = {rbar.r, rbar.u[0], rbar.u[1], rbar.u[2], rbar.e, rbar.p, rbar.h};
+#pragma unroll
+      for (int v = 0; v < 7; ++v) {
+        cl[v] = cn[v];
+        qn[v] = rn[v];
+      }
+    }
+    // Cell i-3 is complete: flush it and slide.
     flush(i - 3, ab[0]);
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
 #pragma unroll
-      for (int v = 0; v < 7; ++v) {
-        sw[k][v] = sw[k + 1][v];
-        ab[k][v] = ab[k + 1][v];
-      }
+      for (int v = 0; v < 7; ++v) sw[k][v] = sw[k + 1][v];
     }
 #pragma unroll
-    for (int v = 0; v < 7; ++v) ab[5][v] = T(0);
+    for (int k = 0; k < 4; ++k) {
+#pragma unroll
+      for (int v = 0; v < 7; ++v) ab[k][v] = ab[k + 1][v];
+    }
+#pragma unroll
+    for (int v = 0; v < 7; ++v) ab[4][v] = T(0);
 #pragma unroll
     for (int v = 0; v < 5; ++v) la[v] = lb[v];
   }
-  // Cells i1-3 .. i1+1 may still hold contributions.
   if (active) {
+    // Cell i1-1: only its left face (face i1-1) belongs to this thread.
+#pragma unroll
+    for (int v = 0; v < 7; ++v) {
+      const T s5[5] = {sw[0][v], sw[1][v], sw[2][v], sw[3][v], sw[4][v]};
+      T sb[5] = {T(0), T(0), T(0), T(0), T(0)};
+      weno5_cell_vjp<T>(s5, T(0), cl[v], sb);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) ab[k][v] += sb[k];
+    }
+    // Cells i1-3 .. i1+1 may still hold contributions.
 #pragma unroll
     for (int k = 0; k < 5; ++k) flush(i1 - 3 + k, ab[k]);
+    if (a.visc) tang_flush(base + (long long)(i1 - 1 + h) * st, gba);
   }
   if (a.visc && a.nu_bar) {
     double m = double(nub);
@@ -627,23 +743,50 @@ __global__ void __launch_bounds__(128) vjp_face_kernel(const VjpArgs a) {
 }
 
 // Conserved cotangents of every cell from its primitive cotangents (the
-// reverse of cons_to_prim), plus the gravity source rho*G*g.
+// reverse of cons_to_prim), plus the gravity source rho*G*g. The y faces'
+// cotangents are read back from the transposed layout through a tile.
 template <typename T>
-__global__ void vjp_cell_kernel(const VjpArgs a) {
-  const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h, nza = a.nz + 2 * a.h;
-  const long long n = (long long)nxa * nya * nza;
+__global__ void __launch_bounds__(256) vjp_cell_kernel(const VjpArgs a) {
+  __shared__ T tile[TT][TT + 1];
+  const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h;
+  const int za = blockIdx.z;
+  const int y0 = blockIdx.x * TT, x0 = blockIdx.y * TT;
+  const int tx = threadIdx.x, ty = threadIdx.y;
   const T gm1 = K<T>::gm1();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int ya = (int)(t % nya);
-    const int xa = (int)((t / nya) % nxa);
-    const int za = (int)(t / ((long long)nya * nxa));
+  T pbs[4][7];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int xa = x0 + ty + 8 * k, ya = y0 + tx;
+    const bool in = xa < nxa && ya < nya;
     const long long o = za * a.sz + xa * a.sx + ya;
-    T c[5], pb[7];
+#pragma unroll
+    for (int v = 0; v < 7; ++v)
+      pbs[k][v] = in ? static_cast<const T*>(a.pbar[v])[o] : T(0);
+  }
+  // tile[y - y0][x - x0], written along x, read along y.
+  for (int v = 0; v < 7; ++v) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int yl = ty + 8 * k;
+      const int xa = x0 + tx, ya = y0 + yl;
+      tile[yl][tx] = (xa < nxa && ya < nya)
+                         ? static_cast<const T*>(a.pbarT[v])[za * a.tsz + ya * a.tsy + xa]
+                         : T(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) pbs[k][v] += tile[tx][ty + 8 * k];
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int xa = x0 + ty + 8 * k, ya = y0 + tx;
+    if (xa >= nxa || ya >= nya) continue;
+    const long long o = za * a.sz + xa * a.sx + ya;
+    T c[5];
+    const T* pb = pbs[k];
 #pragma unroll
     for (int v = 0; v < 5; ++v) c[v] = static_cast<const T*>(a.uk[v])[o];
-#pragma unroll
-    for (int k = 0; k < 7; ++k) pb[k] = static_cast<const T*>(a.pbar[k])[o];
     const T pe = pe_of<T>(a, xa, ya, za);
     const T rho = c[0];
     const T inv = T(1) / rho;
@@ -781,12 +924,10 @@ int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
   const long long cells = (long long)nxa * nya * nza;
   const int pt = 256;
   const unsigned pblocks = (unsigned)std::min<long long>((cells + pt - 1) / pt, 148 * 16);
-  vjp_prim_kernel<T><<<pblocks, pt, 0, s>>>(a);
+  const dim3 tgrid((nya + TT - 1) / TT, (nxa + TT - 1) / TT, nza);
+  const dim3 tblock(TT, 8);
+  vjp_prim_kernel<T><<<tgrid, tblock, 0, s>>>(a);
   note_launch();
-  for (int k = 0; k < 7; ++k) {
-    cudaError_t e = cudaMemsetAsync(a.pbar[k], 0, (size_t)(a.sz * nza) * sizeof(T), s);
-    if (e != cudaSuccess) return record_error(SWC_ERR_LAUNCH, "memset: %s", cudaGetErrorString(e));
-  }
   const int ft = 128;
   for (int D = 0; D < 3; ++D) {
     const int n = D == 0 ? a.nx : (D == 1 ? a.ny : a.nz);
@@ -800,7 +941,7 @@ int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
     else vjp_face_kernel<T, 2><<<blocks, ft, 0, s>>>(a);
     note_launch();
   }
-  vjp_cell_kernel<T><<<pblocks, pt, 0, s>>>(a);
+  vjp_cell_kernel<T><<<tgrid, tblock, 0, s>>>(a);
   note_launch();
   for (int d = 2; d >= 0; --d) {
     VjpHalo hh;
@@ -862,8 +1003,10 @@ extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
       return record_error(SWC_ERR_UNSUPPORTED,
                           "the stage adjoint does not cover primitive BCs");
   }
-  for (int k = 0; k < 14; ++k)
+  for (int k = 0; k < SWC_VJP_SCRATCH; ++k)
     if (!scratch[k]) return record_error(SWC_ERR_ARG, "NULL scratch field %d", k);
+  if (grid->nz + 2 * grid->halo > 65535)
+    return record_error(SWC_ERR_ARG, "stage vjp: nz %d is too large", grid->nz);
   VjpArgs a;
   memset(&a, 0, sizeof(a));
   a.nx = grid->nx; a.ny = grid->ny; a.nz = grid->nz; a.h = grid->halo;
@@ -885,7 +1028,12 @@ extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
   for (int k = 0; k < 7; ++k) {
     a.prim[k] = scratch[k];
     a.pbar[k] = scratch[7 + k];
+    a.primT[k] = scratch[14 + k];
+    a.pbarT[k] = scratch[21 + k];
   }
+  for (int v = 0; v < 5; ++v) a.lamT[v] = scratch[28 + v];
+  a.tsy = grid->nx + 2 * grid->halo;
+  a.tsz = a.tsy * (long long)(grid->ny + 2 * grid->halo);
   for (int d = 0; d < 3; ++d) {
     a.pe[d] = sc->pe_axis[d];
     if (sc->pe_axis[d]) a.has_pe = 1;

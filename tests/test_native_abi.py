@@ -65,6 +65,14 @@ def test_noalloc_limit_matches_header():
   assert m and int(m.group(1)) << int(m.group(2)) == nat.SWC_NOALLOC_MAX_BYTES
 
 
+def test_header_constants_match_python():
+  with open(os.path.join(ROOT, 'include', 'swirlc_b200.h')) as f:
+    text = f.read()
+  for name in ('SWC_VJP_SCRATCH', 'SWC_MAX_OVERRIDES', 'SWC_MAX_FIELDS'):
+    m = re.search(r'#define %s (\d+)' % name, text)
+    assert m and int(m.group(1)) == getattr(nat, name), name
+
+
 def _c_layout():
   src = r'''
 #include <stddef.h>
