@@ -406,27 +406,40 @@ constexpr int TT = 32;
 // cotangent buffers cleared, and lam transposed.
 template <typename T>
 __global__ void __launch_bounds__(256) vjp_prim_kernel(const VjpArgs a) {
-  __shared__ T tile[TT][TT + 1];
+  // Two tiles: variable v goes through tile v % 2, so one barrier per
+  // variable separates its writers from its readers and from the writers
+  // two variables later.
+  __shared__ T tiles[2][TT][TT + 1];
   const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h;
   const int za = blockIdx.z;
   const int y0 = blockIdx.x * TT, x0 = blockIdx.y * TT;
   const int tx = threadIdx.x, ty = threadIdx.y;
+  // All loads first (the stores go to arrays the compiler cannot tell apart
+  // from the loaded ones), then the primitives.
+  T cv[4][5], lv[4][5];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int xa = x0 + ty + 8 * k, ya = y0 + tx;
+    const bool in = xa < nxa && ya < nya;
+    const long long o = za * a.sz + xa * a.sx + ya;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      cv[k][v] = in ? static_cast<const T*>(a.uk[v])[o] : T(1);
+      lv[k][v] = in ? static_cast<const T*>(a.lam[v])[o] : T(0);
+    }
+  }
   T pr[4][7];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-#pragma unroll
-    for (int v = 0; v < 7; ++v) pr[k][v] = T(0);
     const int xa = x0 + ty + 8 * k, ya = y0 + tx;
+    T u, vv, w, e, p, hh;
+    cons_to_prim(cv[k][0], cv[k][1], cv[k][2], cv[k][3], cv[k][4],
+                 pe_of<T>(a, min(xa, nxa - 1), min(ya, nya - 1), za), u, vv,
+                 w, e, p, hh);
+    pr[k][0] = cv[k][0]; pr[k][1] = u; pr[k][2] = vv; pr[k][3] = w;
+    pr[k][4] = e; pr[k][5] = p; pr[k][6] = hh;
     if (xa >= nxa || ya >= nya) continue;
     const long long o = za * a.sz + xa * a.sx + ya;
-    T c[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) c[v] = static_cast<const T*>(a.uk[v])[o];
-    T u, vv, w, e, p, hh;
-    cons_to_prim(c[0], c[1], c[2], c[3], c[4], pe_of<T>(a, xa, ya, za), u,
-                 vv, w, e, p, hh);
-    pr[k][0] = c[0]; pr[k][1] = u; pr[k][2] = vv; pr[k][3] = w;
-    pr[k][4] = e; pr[k][5] = p; pr[k][6] = hh;
 #pragma unroll
     for (int v = 0; v < 7; ++v) {
       static_cast<T*>(a.prim[v])[o] = pr[k][v];
@@ -434,18 +447,12 @@ __global__ void __launch_bounds__(256) vjp_prim_kernel(const VjpArgs a) {
     }
   }
   // tile[x - x0][y - y0]; the transposed write reads it along x.
+#pragma unroll
   for (int v = 0; v < 12; ++v) {
+    T(*tile)[TT + 1] = tiles[v & 1];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      if (v < 7) {
-        tile[ty + 8 * k][tx] = pr[k][v];
-      } else {
-        const int xa = x0 + ty + 8 * k, ya = y0 + tx;
-        tile[ty + 8 * k][tx] =
-            (xa < nxa && ya < nya)
-                ? static_cast<const T*>(a.lam[v - 7])[za * a.sz + xa * a.sx + ya]
-                : T(0);
-      }
+      tile[ty + 8 * k][tx] = v < 7 ? pr[k][v] : lv[k][v - 7];
     }
     __syncthreads();
 #pragma unroll
@@ -461,7 +468,6 @@ __global__ void __launch_bounds__(256) vjp_prim_kernel(const VjpArgs a) {
         static_cast<T*>(a.lamT[v - 7])[ot] = tile[tx][yl];
       }
     }
-    __syncthreads();
   }
 }
 
@@ -747,46 +753,63 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
 // cotangents are read back from the transposed layout through a tile.
 template <typename T>
 __global__ void __launch_bounds__(256) vjp_cell_kernel(const VjpArgs a) {
-  __shared__ T tile[TT][TT + 1];
+  __shared__ T tiles[2][TT][TT + 1];  // as in vjp_prim_kernel
   const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h;
   const int za = blockIdx.z;
   const int y0 = blockIdx.x * TT, x0 = blockIdx.y * TT;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const T gm1 = K<T>::gm1();
-  T pbs[4][7];
+  // Loads first (see vjp_prim_kernel): the cotangents of both layouts and
+  // the state, then the y faces' cotangents through the tile, then lam and
+  // the caller's terms.
+  T pbs[4][7], pbt[4][7], c4[4][5];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int xa = x0 + ty + 8 * k, ya = y0 + tx;
+    const bool in = xa < nxa && ya < nya;
+    const long long o = za * a.sz + xa * a.sx + ya;
+    const int xt = x0 + tx, yt = y0 + ty + 8 * k;
+    const bool int_ = xt < nxa && yt < nya;
+    const long long ot = za * a.tsz + yt * a.tsy + xt;
+#pragma unroll
+    for (int v = 0; v < 7; ++v) {
+      pbs[k][v] = in ? static_cast<const T*>(a.pbar[v])[o] : T(0);
+      pbt[k][v] = int_ ? static_cast<const T*>(a.pbarT[v])[ot] : T(0);
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+      c4[k][v] = in ? static_cast<const T*>(a.uk[v])[o] : T(1);
+  }
+  // tile[y - y0][x - x0], written along x, read along y.
+#pragma unroll
+  for (int v = 0; v < 7; ++v) {
+    T(*tile)[TT + 1] = tiles[v & 1];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) tile[ty + 8 * k][tx] = pbt[k][v];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) pbs[k][v] += tile[tx][ty + 8 * k];
+  }
+  T l4[4][5], x14[4][5], x24[4][5];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const int xa = x0 + ty + 8 * k, ya = y0 + tx;
     const bool in = xa < nxa && ya < nya;
     const long long o = za * a.sz + xa * a.sx + ya;
 #pragma unroll
-    for (int v = 0; v < 7; ++v)
-      pbs[k][v] = in ? static_cast<const T*>(a.pbar[v])[o] : T(0);
-  }
-  // tile[y - y0][x - x0], written along x, read along y.
-  for (int v = 0; v < 7; ++v) {
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int yl = ty + 8 * k;
-      const int xa = x0 + tx, ya = y0 + yl;
-      tile[yl][tx] = (xa < nxa && ya < nya)
-                         ? static_cast<const T*>(a.pbarT[v])[za * a.tsz + ya * a.tsy + xa]
-                         : T(0);
+    for (int v = 0; v < 5; ++v) {
+      l4[k][v] = in ? static_cast<const T*>(a.lam[v])[o] : T(0);
+      x14[k][v] = in && a.x1[v] ? static_cast<const T*>(a.x1[v])[o] : T(0);
+      x24[k][v] = in && a.x2[v] ? static_cast<const T*>(a.x2[v])[o] : T(0);
     }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 4; ++k) pbs[k][v] += tile[tx][ty + 8 * k];
-    __syncthreads();
   }
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const int xa = x0 + ty + 8 * k, ya = y0 + tx;
     if (xa >= nxa || ya >= nya) continue;
     const long long o = za * a.sz + xa * a.sx + ya;
-    T c[5];
+    const T* c = c4[k];
     const T* pb = pbs[k];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) c[v] = static_cast<const T*>(a.uk[v])[o];
     const T pe = pe_of<T>(a, xa, ya, za);
     const T rho = c[0];
     const T inv = T(1) / rho;
@@ -823,107 +846,94 @@ __global__ void __launch_bounds__(256) vjp_cell_kernel(const VjpArgs a) {
 #pragma unroll
       for (int d = 0; d < 3; ++d)
         if (a.gravity_mask & (1 << d))
-          rb += T(a.beta) * static_cast<const T*>(a.lam[1 + d])[o] *
-                K<T>::grav() * T(a.g[d]);
+          rb += T(a.beta) * l4[k][1 + d] * K<T>::grav() * T(a.g[d]);
     }
     out[0] = rb;
+    // The caller's combination on the interior (alpha*lam + c1*x1 + c2*x2):
+    // added before the halo reverse, which is linear and moves only halo
+    // cotangents.
+    if (interior) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v)
+        out[v] += T(a.alpha) * l4[k][v] + T(a.c1) * x14[k][v] +
+                  T(a.c2) * x24[k][v];
+    }
 #pragma unroll
     for (int v = 0; v < 5; ++v) static_cast<T*>(a.vout[v])[o] = out[v];
   }
 }
 
-// Reverse of one dim pass of the halo fill (swc_halo_fill) on vout: the
-// cotangent of every halo cell goes to the cell its value came from and the
-// halo cotangent is cleared (periodic: the wrapped interior layer; Neumann:
-// the edge cell; Dirichlet: nothing).
+// Reverse of the halo fill (swc_halo_fill: x, then y, then z) on vout. The
+// fill is a product of per-dim maps: a halo cell ends up holding the value
+// of the cell (src_x(x), src_y(y), src_z(z)), src_d the identity inside the
+// grid, the wrapped cell (periodic) or the edge cell (Neumann) in the
+// halo, provided every halo dim of the cell is a copy; a Dirichlet (or
+// unfilled) halo dim makes it a value with no source. So each halo cell's
+// cotangent is added to its source cell at once, and cleared. One thread per
+// cell of the padded box (interior threads return at once); several halo
+// cells can share a source (atomics).
 struct VjpHalo {
-  int dim;
   int nx, ny, nz, h;
   long long sx, sz;
   void* f[5];
-  SwcBC bc[5][2];
+  int kind[5][3][2];  // fill kind per field, dim and side
 };
 
 template <typename T>
-__global__ void vjp_halo_kernel(const VjpHalo a) {
-  const int ext[3] = {a.nx + 2 * a.h, a.ny + 2 * a.h, a.nz + 2 * a.h};
-  const long long stride[3] = {a.sx, 1, a.sz};
-  const int d = a.dim;
-  int ax_a, ax_b;
-  if (d == 0) { ax_a = 2; ax_b = 1; }
-  else if (d == 1) { ax_a = 2; ax_b = 0; }
-  else { ax_a = 0; ax_b = 1; }
-  const int na = ext[ax_a], nb = ext[ax_b];
-  const long long plane = (long long)na * nb;
-  const int n = ext[d] - 2 * a.h;
-  const long long total = plane * 2 * 5;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-       t < total; t += (long long)gridDim.x * blockDim.x) {
-    const long long pb = t % plane;
-    const int side = (int)((t / plane) % 2);
-    const int fi = (int)(t / (plane * 2));
-    const int ia = (int)(pb / nb), ib = (int)(pb % nb);
-    const long long base = ia * stride[ax_a] + ib * stride[ax_b];
-    const long long sd = stride[d];
-    T* f = static_cast<T*>(a.f[fi]);
-    const int kind = a.bc[fi][side].kind;
-    for (int l = 0; l < a.h; ++l) {
-      const long long o = side == 0 ? base + (long long)l * sd
-                                    : base + (long long)(n + a.h + l) * sd;
-      const T v = f[o];
-      if (kind == SWC_BC_NONE) continue;
-      f[o] = T(0);
-      long long dst = -1;
-      if (kind == SWC_BC_PERIODIC)
-        dst = side == 0 ? base + (long long)(l + n) * sd
-                        : base + (long long)(a.h + l) * sd;
-      else if (kind == SWC_BC_NEUMANN)
-        dst = side == 0 ? base + (long long)a.h * sd
-                        : base + (long long)(n + a.h - 1) * sd;
-      if (dst < 0) continue;
-      // With n >= 2h the two sides' source cells are disjoint and each
-      // belongs to one thread: a plain update suffices.
-      if (n >= 2 * a.h) f[dst] += v;
-      else atomicAdd(f + dst, v);
-    }
-  }
-}
-
-// Interior: vout = alpha*lam + c1*x1 + c2*x2 + vout; halos: 0.
-template <typename T>
-__global__ void vjp_combine_kernel(const VjpArgs a) {
-  const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h, nza = a.nz + 2 * a.h;
-  const long long n = (long long)nxa * nya * nza;
-  const T al = T(a.alpha), c1 = T(a.c1), c2 = T(a.c2);
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int ya = (int)(t % nya);
-    const int xa = (int)((t / nya) % nxa);
-    const int za = (int)(t / ((long long)nya * nxa));
-    const long long o = za * a.sz + xa * a.sx + ya;
-    const bool interior = xa >= a.h && xa < a.nx + a.h && ya >= a.h &&
-                          ya < a.ny + a.h && za >= a.h && za < a.nz + a.h;
+__global__ void __launch_bounds__(256) vjp_halo_kernel(const VjpHalo a) {
+  const int h = a.h;
+  const int nxa = a.nx + 2 * h, nya = a.ny + 2 * h, nza = a.nz + 2 * h;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nxa * nya * nza) return;
+  const int ya = (int)(t % nya);
+  const long long r = t / nya;
+  const int xa = (int)(r % nxa);
+  const int za = (int)(r / nxa);
+  const int c[3] = {xa, ya, za};
+  const int n[3] = {a.nx, a.ny, a.nz};
+  int side[3];
+  bool halo = false;
 #pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      T* out = static_cast<T*>(a.vout[v]);
-      if (!interior) {
-        out[o] = T(0);
-        continue;
-      }
-      T r = out[o] + al * static_cast<const T*>(a.lam[v])[o];
-      if (a.x1[v]) r += c1 * static_cast<const T*>(a.x1[v])[o];
-      if (a.x2[v]) r += c2 * static_cast<const T*>(a.x2[v])[o];
-      out[o] = r;
+  for (int d = 0; d < 3; ++d) {
+    side[d] = c[d] < h ? 0 : (c[d] >= n[d] + h ? 1 : -1);
+    halo |= side[d] >= 0;
+  }
+  if (!halo) return;
+  const long long o = za * a.sz + xa * a.sx + ya;
+  // All loads first: the stores below go to arrays the compiler cannot
+  // tell apart from the loaded ones.
+  T val[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) val[v] = static_cast<const T*>(a.f[v])[o];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    T* f = static_cast<T*>(a.f[v]);
+    f[o] = T(0);
+    int src[3];
+    bool copy = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      src[d] = c[d];
+      if (side[d] < 0) continue;
+      const int kind = a.kind[v][d][side[d]];
+      if (kind == SWC_BC_PERIODIC)
+        src[d] = side[d] == 0 ? c[d] + n[d] : c[d] - n[d];
+      else if (kind == SWC_BC_NEUMANN)
+        src[d] = side[d] == 0 ? h : n[d] + h - 1;
+      else
+        copy = false;
     }
+    // Sources are interior cells (periodic dims have n >= h, checked by
+    // the caller).
+    if (copy && val[v] != T(0))
+      atomicAdd(f + (long long)src[2] * a.sz + (long long)src[0] * a.sx + src[1],
+                val[v]);
   }
 }
 
 template <typename T>
 int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
   const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h, nza = a.nz + 2 * a.h;
-  const long long cells = (long long)nxa * nya * nza;
-  const int pt = 256;
-  const unsigned pblocks = (unsigned)std::min<long long>((cells + pt - 1) / pt, 148 * 16);
   const dim3 tgrid((nya + TT - 1) / TT, (nxa + TT - 1) / TT, nza);
   const dim3 tblock(TT, 8);
   vjp_prim_kernel<T><<<tgrid, tblock, 0, s>>>(a);
@@ -943,29 +953,25 @@ int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
   }
   vjp_cell_kernel<T><<<tgrid, tblock, 0, s>>>(a);
   note_launch();
-  for (int d = 2; d >= 0; --d) {
+  {
     VjpHalo hh;
     memset(&hh, 0, sizeof(hh));
-    hh.dim = d;
     hh.nx = a.nx; hh.ny = a.ny; hh.nz = a.nz; hh.h = a.h;
     hh.sx = a.sx; hh.sz = a.sz;
     for (int v = 0; v < 5; ++v) {
       hh.f[v] = a.vout[v];
-      const SwcBC& lo = bcs[v].side[d][0];
-      const SwcBC& hi = bcs[v].side[d][1];
-      hh.bc[v][0] = lo;
-      hh.bc[v][1] = hi;
-      if (lo.kind == SWC_BC_PERIODIC || hi.kind == SWC_BC_PERIODIC)
-        hh.bc[v][0].kind = hh.bc[v][1].kind = SWC_BC_PERIODIC;
+      for (int d = 0; d < 3; ++d) {
+        int lo = bcs[v].side[d][0].kind, hi = bcs[v].side[d][1].kind;
+        if (lo == SWC_BC_PERIODIC || hi == SWC_BC_PERIODIC)
+          lo = hi = SWC_BC_PERIODIC;
+        hh.kind[v][d][0] = lo;
+        hh.kind[v][d][1] = hi;
+      }
     }
-    const int ext[3] = {nxa, nya, nza};
-    const long long total = (long long)ext[(d + 1) % 3] * ext[(d + 2) % 3] * 10;
-    const unsigned hb = (unsigned)std::min<long long>((total + 255) / 256, 148 * 16);
-    vjp_halo_kernel<T><<<hb, 256, 0, s>>>(hh);
+    const long long cells = (long long)nxa * nya * nza;
+    vjp_halo_kernel<T><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>(hh);
     note_launch();
   }
-  vjp_combine_kernel<T><<<pblocks, pt, 0, s>>>(a);
-  note_launch();
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? SWC_OK
                           : record_error(SWC_ERR_LAUNCH, "stage vjp: %s",
@@ -1002,6 +1008,14 @@ extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
     if (bcs[v].via_primitive)
       return record_error(SWC_ERR_UNSUPPORTED,
                           "the stage adjoint does not cover primitive BCs");
+    const int nd[3] = {grid->nx, grid->ny, grid->nz};
+    for (int d = 0; d < 3; ++d)
+      if ((bcs[v].side[d][0].kind == SWC_BC_PERIODIC ||
+           bcs[v].side[d][1].kind == SWC_BC_PERIODIC) &&
+          nd[d] < grid->halo)
+        return record_error(SWC_ERR_UNSUPPORTED,
+                            "stage vjp: periodic dim %d has %d cells, fewer "
+                            "than the halo width", d, nd[d]);
   }
   for (int k = 0; k < SWC_VJP_SCRATCH; ++k)
     if (!scratch[k]) return record_error(SWC_ERR_ARG, "NULL scratch field %d", k);
