@@ -31,6 +31,9 @@ struct HaloMember {
   long long sx, sz;
 };
 
+// Halo widths up to this take the path that reads every layer first.
+constexpr int kHaloFast = 8;
+
 // Halo cells of one (field, side, plane position) element t of the pass
 // described by `a` (HaloArgs or HaloMember); t < plane * 2 * a.nf.
 template <typename T, typename A>
@@ -64,6 +67,63 @@ __device__ __forceinline__ void halo_elem(const A& a, long long t) {
       return r == T(0) ? T(0) : f[o] / r;
     };
     auto put = [&](long long o, T val) { f[o] = prim ? rho[o] * val : val; };
+    auto dst = [&](int l) -> long long {
+      return side == 0 ? base + (long long)l * sd
+                       : base + (long long)(n + a.h + l) * sd;
+    };
+    if (a.h <= kHaloFast) {
+      // Every layer's value is read before any is written: the compiler
+      // cannot tell the written cells from the read ones, so reading and
+      // writing layer by layer would cost one memory round trip per layer.
+      T val[kHaloFast];
+      bool set = true;
+      if (bc.kind == SWC_BC_PERIODIC) {
+#pragma unroll
+        for (int l = 0; l < kHaloFast; ++l)
+          if (l < a.h)
+            val[l] = pv(side == 0 ? base + (long long)(l + n) * sd
+                                  : base + (long long)(a.h + l) * sd);
+      } else if (bc.kind == SWC_BC_DIRICHLET) {
+        const T* pl = static_cast<const T*>(bc.planes);
+#pragma unroll
+        for (int l = 0; l < kHaloFast; ++l)
+          if (l < a.h) val[l] = bc.per_layer ? pl[l * plane + pb] : T(bc.value);
+      } else if (bc.kind == SWC_BC_NEUMANN) {
+        // Layer l lies l+1 cells from the edge cell: value -+ (l+1)*inc,
+        // accumulated one layer at a time.
+        const T inc = T(bc.value);
+        T v = pv(side == 0 ? base + (long long)a.h * sd
+                           : base + (long long)(n + a.h - 1) * sd);
+#pragma unroll
+        for (int l = 0; l < kHaloFast; ++l) {
+          v = side == 0 ? v - inc : v + inc;
+          val[l] = v;
+        }
+      } else {
+        set = false;
+      }
+      if (!set) return;
+      // Neumann layer l is cell h-1-l on the low side, n+h+l on the high.
+      auto cell = [&](int l) -> long long {
+        return (bc.kind == SWC_BC_NEUMANN && side == 0)
+                   ? base + (long long)(a.h - 1 - l) * sd
+                   : dst(l);
+      };
+      if (prim) {
+        T r[kHaloFast];
+#pragma unroll
+        for (int l = 0; l < kHaloFast; ++l)
+          if (l < a.h) r[l] = rho[cell(l)];
+#pragma unroll
+        for (int l = 0; l < kHaloFast; ++l)
+          if (l < a.h) f[cell(l)] = r[l] * val[l];
+      } else {
+#pragma unroll
+        for (int l = 0; l < kHaloFast; ++l)
+          if (l < a.h) f[cell(l)] = val[l];
+      }
+      return;
+    }
     if (bc.kind == SWC_BC_PERIODIC) {
       for (int l = 0; l < a.h; ++l) {
         if (side == 0) put(base + l * sd, pv(base + (long long)(l + n) * sd));
@@ -73,8 +133,7 @@ __device__ __forceinline__ void halo_elem(const A& a, long long t) {
       const T* pl = static_cast<const T*>(bc.planes);
       for (int l = 0; l < a.h; ++l) {
         T val = bc.per_layer ? pl[l * plane + pb] : T(bc.value);
-        long long o = side == 0 ? base + l * sd : base + (long long)(n + a.h + l) * sd;
-        put(o, val);
+        put(dst(l), val);
       }
     } else if (bc.kind == SWC_BC_NEUMANN) {
       const T inc = T(bc.value);
