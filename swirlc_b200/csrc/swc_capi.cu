@@ -387,9 +387,51 @@ int swc_halo_fill(const SwcGrid* grid, int32_t dtype, int32_t nfields,
   return SWC_OK;
 }
 
+// SMs of the current device (queried once per device).
+static int sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+      n = 148;
+    cached[dev] = n;
+  }
+  return cached[dev];
+}
+
+// Automatic z segment of the stage kernel for `tiles2d` (y, x) tiles and
+// `per_sm` resident CTAs per SM. A CTA's time is about (zseg + 1) planes
+// (the extra plane: warm-up and the z face below the segment), and the
+// launch takes ceil(CTAs / slots) rounds of them, so the segment count that
+// minimises rounds x (zseg + 1) is taken: at 256^3 that is 8 segments of 32
+// planes (7 rounds of 2048 CTAs on 296 slots) rather than a last round that
+// leaves most SMs idle.
+static int auto_zseg(long long tiles2d, int nz, int per_sm) {
+  const long long slots = (long long)sm_count() * per_sm;
+  long long best_cost = -1;
+  int best = nz;
+  for (int nseg = 1; nseg <= nz; ++nseg) {
+    const int zs = (nz + nseg - 1) / nseg;
+    if (nseg > 1 && zs == (nz + nseg - 2) / (nseg - 1)) continue;  // same zseg
+    if (zs < 4 && nseg > 1) break;
+    const long long segs = (nz + zs - 1) / zs;
+    const long long rounds = (tiles2d * segs + slots - 1) / slots;
+    const long long cost = rounds * (zs + 1);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best = zs;
+    }
+  }
+  return best;
+}
+
 // Checks and the kernel arguments shared by swc_rk_stage and
-// swc_rk_stage_ext; `nf` conserved fields (5 + scalars).
+// swc_rk_stage_ext; `nf` conserved fields (5 + scalars); `per_sm` resident
+// CTAs per SM and the tile's ty extent (x extent 16) size the z segments.
 static int stage_args(const SwcGrid* grid, const SwcScheme* sc, int nf,
+                      int per_sm, int ty,
                       const void* const* uk, const void* const* u0,
                       void* const* uout, int32_t mode, double c0, double c1,
                       const double* dt, double* dtmin_out, StageArgs& a) {
@@ -434,12 +476,11 @@ static int stage_args(const SwcGrid* grid, const SwcScheme* sc, int nf,
   a.limiter = sc->limiter;
   a.nu = sc->nu; a.pr = sc->pr > 0 ? sc->pr : 1.0;
   a.gravity_mask = sc->gravity_mask;
-  // z segment per CTA: enough CTAs for ~4 waves of 2 CTAs/SM, >= 8 planes.
   int zseg = sc->zseg;
   if (zseg <= 0) {
-    long long tiles2d = (long long)((grid->ny + 15) / 16) * ((grid->nx + 15) / 16);
-    long long nseg = std::max<long long>(1, (148 * 2 * 4 + tiles2d - 1) / tiles2d);
-    zseg = (int)std::max<long long>(8, (grid->nz + nseg - 1) / nseg);
+    const long long tiles2d =
+        (long long)((grid->ny + ty - 1) / ty) * ((grid->nx + 15) / 16);
+    zseg = auto_zseg(tiles2d, grid->nz, per_sm);
   }
   a.zseg = std::min(zseg, grid->nz);
   return SWC_OK;
@@ -453,7 +494,8 @@ int swc_rk_stage(const SwcGrid* grid, const SwcScheme* sc,
     return fail(SWC_ERR_UNSUPPORTED,
                 "transported scalars go through swc_rk_stage_ext");
   StageArgs a;
-  int st = stage_args(grid, sc, 5, uk, u0, uout, mode, c0, c1, dt, dtmin_out, a);
+  int st = stage_args(grid, sc, 5, sc && sc->dtype == SWC_F32 ? 2 : 1, 16, uk,
+                      u0, uout, mode, c0, c1, dt, dtmin_out, a);
   if (st) return st;
   const int visc = sc->diffusion ? 1 : 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -526,8 +568,9 @@ int swc_rk_stage_ext(const SwcGrid* grid, const SwcScheme* sc,
                 "Face boundary conditions are not supported with diffusion "
                 "enabled at this time.");
   StageArgs a;
-  int st = stage_args(grid, sc, 5 + ns, uk, u0, uout, mode, c0, c1, dt,
-                      dtmin_out, a);
+  int st = stage_args(grid, sc, 5 + ns, 1,
+                      sc && sc->dtype == SWC_F64 ? 8 : 16, uk, u0, uout, mode,
+                      c0, c1, dt, dtmin_out, a);
   if (st) return st;
   const int visc = sc->diffusion ? 1 : 0;
   const int help = e.p_ref ? 1 : 0;

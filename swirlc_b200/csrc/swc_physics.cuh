@@ -8,13 +8,6 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-// 1: single-precision WENO runs the neg/pos pair as f32x2 instructions
-// (measured slower on B200: operand-pair moves outweigh the halved FP32
-// issue count, so the scalar form is the default).
-#ifndef SWC_PACKED_WENO
-#define SWC_PACKED_WENO 0
-#endif
-
 namespace swc {
 
 // physics/constant.py:17-41. Python doubles rounded once to T, as TF does
@@ -41,6 +34,12 @@ __device__ __forceinline__ T dnn(T x, T y) {  // tf.math.divide_no_nan
 // reciprocal approximation (<= 1 ulp) and x/y the 2-ulp division.
 __device__ __forceinline__ float rcp_(float x) { return 1.0f / x; }
 __device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
+// x / y by a divisor y fixed for the whole launch, with ry = rcp_(y) formed
+// once: the single-precision quotient under -use_fast_math is x * (1/y) with
+// the hardware reciprocal, i.e. this product; double precision keeps the
+// correctly rounded quotient.
+__device__ __forceinline__ float divk(float x, float /*y*/, float ry) { return x * ry; }
+__device__ __forceinline__ double divk(double x, double y, double /*ry*/) { return x / y; }
 __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
 __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
 __device__ __forceinline__ float min_(float a, float b) { return fminf(a, b); }
@@ -288,99 +287,268 @@ __device__ __forceinline__ void reconstruct_cell(const T* s, int limiter,
 }
 
 // ---------------------------------------------------------------------------
-// Packed single-precision reconstruction. The neg value of face i-1/2 (right
-// face of cell i-1) and its pos value (left face of cell i) use the same
-// formulas on stencils shifted by one cell, with mirrored coefficients, so
-// both run as one sequence of Blackwell f32x2 instructions (FFMA2 / FADD2 /
-// FMUL2): lane x = neg, lane y = pos.
+// Lane-generic reconstruction used by the fused stage. Face reconstruction
+// applies the same formulas to every variable on the same stencil cells, so
+// two variables share one instruction stream: Two<float> runs them as
+// Blackwell f32x2 instructions (FFMA2 / FADD2 / FMUL2 issue both lanes in one
+// slot), Two<double> as two scalar lanes, One<T> is a single variable. Every
+// product and sum is rounded as written (no contraction), so a value comes
+// out bit for bit the same whichever lane count, call site or form (face
+// pair or cell-centred) computes it. Reciprocals run per lane.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
-  return __ffma2_rn(a, b, c);
+template <typename T>
+struct One;
+template <>
+struct One<float> {
+  using S = float;
+  using V = float;
+  static __device__ __forceinline__ V splat(float a) { return a; }
+  static __device__ __forceinline__ V fma(V a, V b, V c) { return __fmaf_rn(a, b, c); }
+  static __device__ __forceinline__ V mul(V a, V b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ V add(V a, V b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ V sub(V a, V b) { return __fsub_rn(a, b); }
+  static __device__ __forceinline__ V rcp(V a) { return 1.0f / a; }
+  template <class F>
+  static __device__ __forceinline__ V map3(F f, V a, V b, V c) { return f(a, b, c); }
+};
+template <>
+struct One<double> {
+  using S = double;
+  using V = double;
+  static __device__ __forceinline__ V splat(double a) { return a; }
+  static __device__ __forceinline__ V fma(V a, V b, V c) { return __fma_rn(a, b, c); }
+  static __device__ __forceinline__ V mul(V a, V b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ V add(V a, V b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ V sub(V a, V b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ V rcp(V a) { return 1.0 / a; }
+  template <class F>
+  static __device__ __forceinline__ V map3(F f, V a, V b, V c) { return f(a, b, c); }
+};
+template <typename T>
+struct Two;
+template <>
+struct Two<float> {
+  using S = float;
+  using V = float2;
+  static __device__ __forceinline__ V mk(float a, float b) { return make_float2(a, b); }
+  static __device__ __forceinline__ V splat(float a) { return make_float2(a, a); }
+  static __device__ __forceinline__ V fma(V a, V b, V c) { return __ffma2_rn(a, b, c); }
+  static __device__ __forceinline__ V mul(V a, V b) { return __fmul2_rn(a, b); }
+  static __device__ __forceinline__ V add(V a, V b) { return __fadd2_rn(a, b); }
+  // a - b, rounded once (b * -1 is exact).
+  static __device__ __forceinline__ V sub(V a, V b) { return __ffma2_rn(b, splat(-1.0f), a); }
+  static __device__ __forceinline__ V rcp(V a) { return make_float2(1.0f / a.x, 1.0f / a.y); }
+  template <class F>
+  static __device__ __forceinline__ V map3(F f, V a, V b, V c) {
+    return make_float2(f(a.x, b.x, c.x), f(a.y, b.y, c.y));
+  }
+};
+template <>
+struct Two<double> {
+  using S = double;
+  using V = double2;
+  static __device__ __forceinline__ V mk(double a, double b) { return make_double2(a, b); }
+  static __device__ __forceinline__ V splat(double a) { return make_double2(a, a); }
+  static __device__ __forceinline__ V fma(V a, V b, V c) {
+    return make_double2(__fma_rn(a.x, b.x, c.x), __fma_rn(a.y, b.y, c.y));
+  }
+  static __device__ __forceinline__ V mul(V a, V b) {
+    return make_double2(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y));
+  }
+  static __device__ __forceinline__ V add(V a, V b) {
+    return make_double2(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y));
+  }
+  static __device__ __forceinline__ V sub(V a, V b) {
+    return make_double2(__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y));
+  }
+  static __device__ __forceinline__ V rcp(V a) { return make_double2(1.0 / a.x, 1.0 / a.y); }
+  template <class F>
+  static __device__ __forceinline__ V map3(F f, V a, V b, V c) {
+    return make_double2(f(a.x, b.x, c.x), f(a.y, b.y, c.y));
+  }
+};
+
+// WENO5-JS on the cell stencil v[c-2..c+2]: the reciprocals
+// i_r = 1/(eps + beta_r)^2 of the three candidate stencils (shared by both
+// faces of the cell), then the value on the right face (c+1/2, linear
+// weights d = (0.3, 0.6, 0.1)) and on the left face (c-1/2, d mirrored);
+// candidate polynomials of the reference prototype's `weno5`.
+template <class O>
+struct Weno5Inv {
+  typename O::V i0, i1, i2;
+};
+template <class O>
+__device__ __forceinline__ typename O::V weno5_beta(typename O::V a,
+                                                    typename O::V b) {
+  using S = typename O::S;
+  return O::fma(O::mul(O::splat(S(13.0 / 12.0)), a), a,
+                O::mul(O::mul(O::splat(S(0.25)), b), b));
 }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 rcp2(float2 a) {
-  return make_float2(1.0f / a.x, 1.0f / a.y);
+template <class O>
+__device__ __forceinline__ Weno5Inv<O> weno5_inv(
+    typename O::V vm2, typename O::V vm1, typename O::V v0, typename O::V vp1,
+    typename O::V vp2) {
+  using S = typename O::S;
+  using V = typename O::V;
+  const V m2 = O::splat(S(-2)), k3 = O::splat(S(3)), m4 = O::splat(S(-4));
+  const V eps = O::splat(S(1e-6));
+  V b0 = weno5_beta<O>(O::add(O::fma(m2, vp1, v0), vp2),
+                       O::fma(m4, vp1, O::fma(k3, v0, vp2)));
+  V b1 = weno5_beta<O>(O::add(O::fma(m2, v0, vm1), vp1), O::sub(vm1, vp1));
+  V b2 = weno5_beta<O>(O::add(O::fma(m2, vm1, vm2), v0),
+                       O::fma(k3, v0, O::fma(m4, vm1, vm2)));
+  b0 = O::add(b0, eps);
+  b1 = O::add(b1, eps);
+  b2 = O::add(b2, eps);
+  return {O::rcp(O::mul(b0, b0)), O::rcp(O::mul(b1, b1)),
+          O::rcp(O::mul(b2, b2))};
+}
+template <class O>
+__device__ __forceinline__ typename O::V weno5_right_v(
+    const Weno5Inv<O>& w, typename O::V vm2, typename O::V vm1,
+    typename O::V v0, typename O::V vp1, typename O::V vp2) {
+  using S = typename O::S;
+  using V = typename O::V;
+  const V a0 = O::mul(O::splat(S(0.3)), w.i0);
+  const V a1 = O::mul(O::splat(S(0.6)), w.i1);
+  const V a2 = O::mul(O::splat(S(0.1)), w.i2);
+  const V q0 = O::fma(O::splat(S(-1.0 / 6.0)), vp2,
+                      O::fma(O::splat(S(5.0 / 6.0)), vp1,
+                             O::mul(O::splat(S(1.0 / 3.0)), v0)));
+  const V q1 = O::fma(O::splat(S(1.0 / 3.0)), vp1,
+                      O::fma(O::splat(S(5.0 / 6.0)), v0,
+                             O::mul(O::splat(S(-1.0 / 6.0)), vm1)));
+  const V q2 = O::fma(O::splat(S(11.0 / 6.0)), v0,
+                      O::fma(O::splat(S(-7.0 / 6.0)), vm1,
+                             O::mul(O::splat(S(1.0 / 3.0)), vm2)));
+  const V num = O::fma(a2, q2, O::fma(a1, q1, O::mul(a0, q0)));
+  return O::mul(num, O::rcp(O::add(O::add(a0, a1), a2)));
+}
+template <class O>
+__device__ __forceinline__ typename O::V weno5_left_v(
+    const Weno5Inv<O>& w, typename O::V vm2, typename O::V vm1,
+    typename O::V v0, typename O::V vp1, typename O::V vp2) {
+  using S = typename O::S;
+  using V = typename O::V;
+  const V a0 = O::mul(O::splat(S(0.1)), w.i0);
+  const V a1 = O::mul(O::splat(S(0.6)), w.i1);
+  const V a2 = O::mul(O::splat(S(0.3)), w.i2);
+  const V q0 = O::fma(O::splat(S(1.0 / 3.0)), vp2,
+                      O::fma(O::splat(S(-7.0 / 6.0)), vp1,
+                             O::mul(O::splat(S(11.0 / 6.0)), v0)));
+  const V q1 = O::fma(O::splat(S(-1.0 / 6.0)), vp1,
+                      O::fma(O::splat(S(5.0 / 6.0)), v0,
+                             O::mul(O::splat(S(1.0 / 3.0)), vm1)));
+  const V q2 = O::fma(O::splat(S(1.0 / 3.0)), v0,
+                      O::fma(O::splat(S(5.0 / 6.0)), vm1,
+                             O::mul(O::splat(S(-1.0 / 6.0)), vm2)));
+  const V num = O::fma(a2, q2, O::fma(a1, q1, O::mul(a0, q0)));
+  return O::mul(num, O::rcp(O::add(O::add(a0, a1), a2)));
 }
 
-// WENO5-JS pair from the 6-cell stencil s[0..5] = v[i-3..i+2].
-__device__ __forceinline__ float2 weno5_pair(const float* s) {
-  const float2 vm2 = f2(s[0], s[1]), vm1 = f2(s[1], s[2]), v0 = f2(s[2], s[3]);
-  const float2 vp1 = f2(s[3], s[4]), vp2 = f2(s[4], s[5]);
-  const float2 k1312 = f2(13.0f / 12.0f, 13.0f / 12.0f);
-  const float2 kq = f2(0.25f, 0.25f), eps = f2(1e-6f, 1e-6f);
-  const float2 m2 = f2(-2.0f, -2.0f), k3 = f2(3.0f, 3.0f), m4 = f2(-4.0f, -4.0f);
-  // beta_0 on (v0, vp1, vp2)
-  float2 a = add2(fma2(m2, vp1, v0), vp2);
-  float2 b = fma2(m4, vp1, fma2(k3, v0, vp2));
-  float2 b0 = fma2(mul2(k1312, a), a, mul2(mul2(kq, b), b));
-  // beta_1 on (vm1, v0, vp1)
-  a = add2(fma2(m2, v0, vm1), vp1);
-  b = add2(vm1, mul2(f2(-1.0f, -1.0f), vp1));
-  float2 b1 = fma2(mul2(k1312, a), a, mul2(mul2(kq, b), b));
-  // beta_2 on (vm2, vm1, v0)
-  a = add2(fma2(m2, vm1, vm2), v0);
-  b = fma2(k3, v0, fma2(m4, vm1, vm2));
-  float2 b2 = fma2(mul2(k1312, a), a, mul2(mul2(kq, b), b));
-  b0 = add2(b0, eps);
-  b1 = add2(b1, eps);
-  b2 = add2(b2, eps);
-  // alpha_r = d_r / (eps + beta_r)^2; d = (0.3, 0.6, 0.1) for neg and the
-  // mirror (0.1, 0.6, 0.3) for pos.
-  const float2 a0 = mul2(f2(0.3f, 0.1f), rcp2(mul2(b0, b0)));
-  const float2 a1 = mul2(f2(0.6f, 0.6f), rcp2(mul2(b1, b1)));
-  const float2 a2 = mul2(f2(0.1f, 0.3f), rcp2(mul2(b2, b2)));
-  // Candidates: neg = right face of the cell, pos = left face.
-  const float2 q0 = fma2(f2(-1.0f / 6.0f, 1.0f / 3.0f), vp2,
-                         fma2(f2(5.0f / 6.0f, -7.0f / 6.0f), vp1,
-                              mul2(f2(1.0f / 3.0f, 11.0f / 6.0f), v0)));
-  const float2 q1 = fma2(f2(1.0f / 3.0f, -1.0f / 6.0f), vp1,
-                         fma2(f2(5.0f / 6.0f, 5.0f / 6.0f), v0,
-                              mul2(f2(-1.0f / 6.0f, 1.0f / 3.0f), vm1)));
-  const float2 q2 = fma2(f2(11.0f / 6.0f, 1.0f / 3.0f), v0,
-                         fma2(f2(-7.0f / 6.0f, 5.0f / 6.0f), vm1,
-                              mul2(f2(1.0f / 3.0f, -1.0f / 6.0f), vm2)));
-  const float2 num = fma2(a2, q2, fma2(a1, q1, mul2(a0, q0)));
-  const float2 den = add2(add2(a0, a1), a2);
-  return mul2(num, rcp2(den));
+// WENO3 (k = 2) on v[c-1..c+1]: reciprocals of (eps + beta_r)^2, then the
+// right face (d = (2/3, 1/3), candidates (1/2, 1/2) and (-1/2, 3/2)) or the
+// left face (d mirrored).
+template <class O>
+__device__ __forceinline__ void weno3_inv(typename O::V vm1, typename O::V v0,
+                                          typename O::V vp1, typename O::V& i0,
+                                          typename O::V& i1) {
+  using S = typename O::S;
+  using V = typename O::V;
+  const V d0 = O::sub(vp1, v0), d1 = O::sub(v0, vm1);
+  const V eps = O::splat(S(1e-6));
+  const V b0 = O::add(O::mul(d0, d0), eps), b1 = O::add(O::mul(d1, d1), eps);
+  i0 = O::rcp(O::mul(b0, b0));
+  i1 = O::rcp(O::mul(b1, b1));
+}
+template <class O>
+__device__ __forceinline__ typename O::V weno3_side_v(
+    typename O::V i0, typename O::V i1, typename O::V vm1, typename O::V v0,
+    typename O::V vp1, bool right) {
+  using S = typename O::S;
+  using V = typename O::V;
+  const V h = O::splat(S(0.5)), mh = O::splat(S(-0.5)), k15 = O::splat(S(1.5));
+  const V a0 = O::mul(O::splat(right ? S(2.0 / 3.0) : S(1.0 / 3.0)), i0);
+  const V a1 = O::mul(O::splat(right ? S(1.0 / 3.0) : S(2.0 / 3.0)), i1);
+  const V q0 = right ? O::fma(h, vp1, O::mul(h, v0)) : O::fma(mh, vp1, O::mul(k15, v0));
+  const V q1 = right ? O::fma(k15, v0, O::mul(mh, vm1)) : O::fma(h, v0, O::mul(h, vm1));
+  return O::mul(O::fma(a1, q1, O::mul(a0, q0)), O::rcp(O::add(a0, a1)));
 }
 
-// WENO3-JS pair from s[0..3] = v[i-2..i+1].
-__device__ __forceinline__ float2 weno3_pair(const float* s) {
-  const float2 vm1 = f2(s[0], s[1]), v0 = f2(s[1], s[2]), vp1 = f2(s[2], s[3]);
-  const float2 eps = f2(1e-6f, 1e-6f);
-  float2 d0 = add2(vp1, mul2(f2(-1.0f, -1.0f), v0));
-  float2 d1 = add2(v0, mul2(f2(-1.0f, -1.0f), vm1));
-  float2 b0 = fma2(d0, d0, eps), b1 = fma2(d1, d1, eps);
-  const float2 a0 = mul2(f2(2.0f / 3.0f, 1.0f / 3.0f), rcp2(mul2(b0, b0)));
-  const float2 a1 = mul2(f2(1.0f / 3.0f, 2.0f / 3.0f), rcp2(mul2(b1, b1)));
-  const float2 q0 = fma2(f2(0.5f, -0.5f), vp1, mul2(f2(0.5f, 1.5f), v0));
-  const float2 q1 = fma2(f2(1.5f, 0.5f), v0, mul2(f2(-0.5f, 0.5f), vm1));
-  return mul2(fma2(a1, q1, mul2(a0, q0)), rcp2(add2(a0, a1)));
+// MUSCL slopes per lane (muscl_slope).
+template <class O>
+__device__ __forceinline__ typename O::V muscl_slope_v(typename O::V vm1,
+                                                       typename O::V v0,
+                                                       typename O::V vp1,
+                                                       int limiter) {
+  using S = typename O::S;
+  return O::map3([limiter](S a, S b, S c) { return muscl_slope(a, b, c, limiter); },
+                 vm1, v0, vp1);
+}
+
+// Face i-1/2 from s[k] = v[i-LO+k] (Stencil<SCHEME>): neg from cell i-1
+// (its right face), pos from cell i (its left face).
+template <int SCHEME, class O>
+__device__ __forceinline__ void recon_face(const typename O::V* s, int limiter,
+                                           typename O::V& neg,
+                                           typename O::V& pos) {
+  using S = typename O::S;
+  if constexpr (SCHEME == 0) {
+    neg = weno5_right_v<O>(weno5_inv<O>(s[0], s[1], s[2], s[3], s[4]), s[0],
+                           s[1], s[2], s[3], s[4]);
+    pos = weno5_left_v<O>(weno5_inv<O>(s[1], s[2], s[3], s[4], s[5]), s[1],
+                          s[2], s[3], s[4], s[5]);
+  } else if constexpr (SCHEME == 1) {
+    typename O::V i0, i1;
+    weno3_inv<O>(s[0], s[1], s[2], i0, i1);
+    neg = weno3_side_v<O>(i0, i1, s[0], s[1], s[2], true);
+    weno3_inv<O>(s[1], s[2], s[3], i0, i1);
+    pos = weno3_side_v<O>(i0, i1, s[1], s[2], s[3], false);
+  } else if constexpr (SCHEME == 2) {
+    neg = O::fma(O::splat(S(0.5)), muscl_slope_v<O>(s[0], s[1], s[2], limiter), s[1]);
+    pos = O::fma(O::splat(S(-0.5)), muscl_slope_v<O>(s[1], s[2], s[3], limiter), s[2]);
+  } else {
+    neg = s[0];
+    pos = s[0];
+  }
+}
+
+// Both faces of cell c from s[k] = v[c-CL+k] (CellStencil<SCHEME>): `left`
+// is the pos value of face c-1/2, `right` the neg value of face c+1/2, bit
+// for bit what recon_face gives for them.
+template <int SCHEME, class O>
+__device__ __forceinline__ void recon_cell(const typename O::V* s, int limiter,
+                                           typename O::V& left,
+                                           typename O::V& right) {
+  using S = typename O::S;
+  if constexpr (SCHEME == 0) {
+    const Weno5Inv<O> w = weno5_inv<O>(s[0], s[1], s[2], s[3], s[4]);
+    right = weno5_right_v<O>(w, s[0], s[1], s[2], s[3], s[4]);
+    left = weno5_left_v<O>(w, s[0], s[1], s[2], s[3], s[4]);
+  } else if constexpr (SCHEME == 1) {
+    typename O::V i0, i1;
+    weno3_inv<O>(s[0], s[1], s[2], i0, i1);
+    right = weno3_side_v<O>(i0, i1, s[0], s[1], s[2], true);
+    left = weno3_side_v<O>(i0, i1, s[0], s[1], s[2], false);
+  } else if constexpr (SCHEME == 2) {
+    const typename O::V sl = muscl_slope_v<O>(s[0], s[1], s[2], limiter);
+    right = O::fma(O::splat(S(0.5)), sl, s[1]);
+    left = O::fma(O::splat(S(-0.5)), sl, s[1]);
+  } else {
+    left = s[0];
+    right = s[1];
+  }
 }
 
 template <int SCHEME, typename T>
 __device__ __forceinline__ void reconstruct(const T* s, int limiter, T& neg,
                                             T& pos) {
   if constexpr (SCHEME == 0) {
-    if constexpr (sizeof(T) == 4 && SWC_PACKED_WENO) {
-      float2 r = weno5_pair(s);
-      neg = r.x;
-      pos = r.y;
-    } else {
-      neg = weno5_right(s[0], s[1], s[2], s[3], s[4]);
-      pos = weno5_left(s[1], s[2], s[3], s[4], s[5]);
-    }
+    neg = weno5_right(s[0], s[1], s[2], s[3], s[4]);
+    pos = weno5_left(s[1], s[2], s[3], s[4], s[5]);
   } else if constexpr (SCHEME == 1) {
-    if constexpr (sizeof(T) == 4 && SWC_PACKED_WENO) {
-      float2 r = weno3_pair(s);
-      neg = r.x;
-      pos = r.y;
-    } else {
-      neg = weno3_right(s[0], s[1], s[2]);
-      pos = weno3_left(s[1], s[2], s[3]);
-    }
+    neg = weno3_right(s[0], s[1], s[2]);
+    pos = weno3_left(s[1], s[2], s[3]);
   } else if constexpr (SCHEME == 2) {
     neg = s[1] + T(0.5) * muscl_slope(s[0], s[1], s[2], limiter);
     pos = s[2] - T(0.5) * muscl_slope(s[1], s[2], s[3], limiter);
@@ -582,11 +750,11 @@ __device__ __forceinline__ void scalar_fluxes(const Prim<T>& l,
 template <typename T, int D>
 __device__ __forceinline__ void viscous_flux(
     T ra, T rb, const T* ua, const T* ub, T pa, T pb, const T ga[3][3],
-    const T gb[3][3], T h_d, T nu, T inv_pr, T* f) {
-  // Backward differences along D of u, v, w and T = p/(rho R).
+    const T gb[3][3], T h_d, T rh_d, T nu, T inv_pr, T* f) {
+  // Backward differences along D of u, v, w and T = p/(rho R); rh_d = 1/h_d.
   T bd[3];
 #pragma unroll
-  for (int c = 0; c < 3; ++c) bd[c] = (ub[c] - ua[c]) / h_d;
+  for (int c = 0; c < 3; ++c) bd[c] = divk(ub[c] - ua[c], h_d, rh_d);
   // div on face D: bwd_D(u_D) + sum over t != D of lin(central_t(u_t)).
   T g[3];  // g[c] = d u_c / d x_c on face D
 #pragma unroll
@@ -613,7 +781,7 @@ __device__ __forceinline__ void viscous_flux(
   T tb = pb / (rb * K<T>::r_gas());
   T ka = inv_pr * K<T>::cp() * (nu * ra);
   T kb = inv_pr * K<T>::cp() * (nu * rb);
-  T q = -(T(0.5) * (ka + kb)) * ((tb - ta) / h_d);
+  T q = -(T(0.5) * (ka + kb)) * divk(tb - ta, h_d, rh_d);
   T dot = uf[0] * tau[0] + uf[1] * tau[1] + uf[2] * tau[2];
 #pragma unroll
   for (int c = 0; c < 3; ++c) f[1 + c] = f[1 + c] + (-tau[c]);

@@ -16,6 +16,8 @@
 // computed exactly once per CTA.
 #pragma once
 
+#include <type_traits>
+
 #include "swc_physics.cuh"
 #include "swirlc_b200.h"
 
@@ -50,28 +52,23 @@ __device__ __forceinline__ void atomic_min_pos(double* addr, double v) {
             static_cast<unsigned long long>(__double_as_longlong(v)));
 }
 
-template <typename T>
-__device__ __forceinline__ void set_var(Prim<T>& q, int v, T x) {
-  switch (v) {
-    case 0: q.r = x; break;
-    case 1: q.u[0] = x; break;
-    case 2: q.u[1] = x; break;
-    case 3: q.u[2] = x; break;
-    case 4: q.e = x; break;
-    case 5: q.p = x; break;
-    default: q.h = x; break;
-  }
-}
-
 template <int SCHEME, bool VISC>
 struct Geom {
   static constexpr int LO = Stencil<SCHEME>::LO;
   static constexpr int RI = Stencil<SCHEME>::RI;
   static constexpr int NW = LO + RI;
+  // Cell-centred stencil v[c-CL .. c+CR] (z faces).
+  static constexpr int CL = CellStencil<SCHEME>::CL;
+  static constexpr int CR = CellStencil<SCHEME>::CR;
+  static constexpr int CW = CL + CR + 1;
   static constexpr int cmax(int a, int b) { return a > b ? a : b; }
+  static constexpr int NOFF = cmax(NW, CW);
   static constexpr int HR = cmax(cmax(LO, RI - 1), VISC ? 1 : 0);
-  static constexpr int ZLO = cmax(cmax(LO - 1, VISC ? 1 : 0), 0);
-  static constexpr int ZHI = cmax(cmax(RI, VISC ? 1 : 0), 1);
+  // Planes below / above the centre plane zc held in the ring: the cell
+  // above (zc+1) is reconstructed along z while zc is processed, and the
+  // first pass of a segment also reconstructs its own plane.
+  static constexpr int ZLO = cmax(cmax(cmax(LO - 1, CL), VISC ? 1 : 0), 0);
+  static constexpr int ZHI = cmax(cmax(cmax(RI, CR + 1), VISC ? 1 : 0), 1);
   static constexpr int RING = ZLO + 1 + ZHI;
   // Halo layers the stored arrays need.
   static constexpr int NEED = cmax(HR, cmax(ZLO + 1, ZHI));
@@ -133,7 +130,8 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
   using L = Layout<T, SCHEME, VISC, TY, TX, NS, HELP>;
   constexpr int NV = L::NV, NCS = L::NCS, NF = L::NF;
   constexpr int LO = G::LO, NW = G::NW, HR = G::HR, ZLO = G::ZLO,
-                ZHI = G::ZHI, RING = G::RING;
+                ZHI = G::ZHI, RING = G::RING, CL = G::CL, CW = G::CW,
+                NOFF = G::NOFF;
   constexpr int PW = L::PW, PH = L::PH, PS = L::PS, NT = L::NT, PER = L::PER;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -262,43 +260,92 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
   //   ta/tb    ring offsets of the t1-/t1+/t2-/t2+ neighbours of the cells
   //            a = i-1 and b = i (viscous cross derivatives)
   auto hsel = [&](int d) -> T { return d == 0 ? dx : (d == 1 ? dy : dz); };
+  // Reciprocals of the launch-constant divisors h_d and 2 h_d.
+  const T rdx = rcp_(dx), rdy = rcp_(dy), rdz = rcp_(dz);
+  const T r2dx = rcp_(T(2) * dx), r2dy = rcp_(T(2) * dy), r2dz = rcp_(T(2) * dz);
+  auto rsel = [&](int d) -> T { return d == 0 ? rdx : (d == 1 ? rdy : rdz); };
+  auto r2sel = [&](int d) -> T { return d == 0 ? r2dx : (d == 1 ? r2dy : r2dz); };
   //   bside    EXT only: -1, or the side (0 low, 1 high) of the grid boundary
   //            this face lies on; pidx its index in a face plane [A][B]
   constexpr int NSA = NS > 0 ? NS : 1;
-  auto face = [&](int dn, const int* off, const int* ta, const int* tb, T pe,
-                  int bside, long long pidx, T* f) {
+  // Every ring variable reconstructed at the ring offsets off[k]: with
+  // CELL false the face form (stencil v[i-LO..i+RI-1] of face i-1/2; lo =
+  // neg, hi = pos), with CELL true the cell form (stencil v[c-CL..c+CR]; lo
+  // = value on the cell's lower face, hi = on its upper face). vel[] maps
+  // the rotated velocity slots to ring variables. The 7 primitives run as
+  // the pairs (rho, e), (u_n, u_t1), (u_t2, p) and h alone; each pair is
+  // one two-lane instruction stream.
+  auto recon_all = [&](auto cell_tag, const int* off, const int* vel,
+                       Prim<T>& lo, Prim<T>& hi, T* phlo, T* phhi, T& pdlo,
+                       T& pdhi) {
+    constexpr bool CELL = decltype(cell_tag)::value;
+    constexpr int NK = CELL ? CW : NW;
+    using O2 = Two<T>;
+    using O1 = One<T>;
+    using V2 = typename O2::V;
+    const int va[3] = {0, vel[0], vel[2]};
+    const int vb[3] = {4, vel[1], 5};
+    V2 rl[3], rh[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const T* ba = ring + va[j] * PS;
+      const T* bb = ring + vb[j] * PS;
+      V2 sv[NK];
+#pragma unroll
+      for (int k = 0; k < NK; ++k) sv[k] = O2::mk(ba[off[k]], bb[off[k]]);
+      if constexpr (CELL) recon_cell<SCHEME, O2>(sv, a.limiter, rl[j], rh[j]);
+      else recon_face<SCHEME, O2>(sv, a.limiter, rl[j], rh[j]);
+    }
+    lo.r = rl[0].x; lo.e = rl[0].y; lo.u[0] = rl[1].x;
+    lo.u[1] = rl[1].y; lo.u[2] = rl[2].x; lo.p = rl[2].y;
+    hi.r = rh[0].x; hi.e = rh[0].y; hi.u[0] = rh[1].x;
+    hi.u[1] = rh[1].y; hi.u[2] = rh[2].x; hi.p = rh[2].y;
+    auto one = [&](int var, T& l, T& r) {
+      const T* base = ring + var * PS;
+      T sv[NK];
+#pragma unroll
+      for (int k = 0; k < NK; ++k) sv[k] = base[off[k]];
+      if constexpr (CELL) recon_cell<SCHEME, O1>(sv, a.limiter, l, r);
+      else recon_face<SCHEME, O1>(sv, a.limiter, l, r);
+    };
+    one(6, lo.h, hi.h);
+#pragma unroll
+    for (int q = 0; q < NS; ++q) one(7 + q, phlo[q], phhi[q]);
+    if constexpr (HELP) {
+      one(7 + NS, pdlo, pdhi);
+    } else {
+      pdlo = lo.p;
+      pdhi = hi.p;
+    }
+  };
+  // z faces: the lower state of the face above plane zc is the upper-face
+  // value of cell zc, carried from the previous plane's reconstruction.
+  Prim<T> zq;
+  T zph[NSA], zpd;
+  auto face = [&](int dn, const int* off, int oa, int ob, const int* ta,
+                  const int* tb, T pe, int bside, long long pidx, T* f) {
     const int t1 = dn == 0 ? 1 : 0, t2 = dn == 2 ? 1 : 2;
     const int vel[3] = {1 + dn, 1 + t1, 1 + t2};
     Prim<T> ql, qr;
-#pragma unroll
-    for (int v = 0; v < 7; ++v) {
-      int vv = v;
-      if (v >= 1 && v <= 3) vv = vel[v - 1];
-      const T* base = ring + vv * PS;
-      T s[NW];
-#pragma unroll
-      for (int k = 0; k < NW; ++k) s[k] = base[off[k]];
-      T ng, ps;
-      reconstruct<SCHEME>(s, a.limiter, ng, ps);
-      set_var(ql, v, ng);
-      set_var(qr, v, ps);
-    }
     T phl[NSA], phr[NSA];
+    T pdl, pdr;
+    if (dn == 2) {
+      // off[] is the cell stencil of cell zc+1: its lower-face value is the
+      // upper state of this face, its upper-face value carries on.
+      Prim<T> up;
+      T phu[NSA], pdu;
+      recon_all(std::true_type{}, off, vel, qr, up, phr, phu, pdr, pdu);
+      ql = zq;
+      zq = up;
 #pragma unroll
-    for (int q = 0; q < NS; ++q) {
-      const T* base = ring + (7 + q) * PS;
-      T s[NW];
-#pragma unroll
-      for (int k = 0; k < NW; ++k) s[k] = base[off[k]];
-      reconstruct<SCHEME>(s, a.limiter, phl[q], phr[q]);
-    }
-    T pdl = ql.p, pdr = qr.p;
-    if constexpr (HELP) {
-      const T* base = ring + (7 + NS) * PS;
-      T s[NW];
-#pragma unroll
-      for (int k = 0; k < NW; ++k) s[k] = base[off[k]];
-      reconstruct<SCHEME>(s, a.limiter, pdl, pdr);
+      for (int q = 0; q < NS; ++q) {
+        phl[q] = zph[q];
+        zph[q] = phu[q];
+      }
+      pdl = zpd;
+      zpd = pdu;
+    } else {
+      recon_all(std::false_type{}, off, vel, ql, qr, phl, phr, pdl, pdr);
     }
     auto plane_val = [&](const SwcOverride& o) -> T {
       return o.plane ? static_cast<const T*>(o.plane)[pidx] : T(o.value);
@@ -380,7 +427,6 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
       for (int q = 0; q < NSA; ++q) fvs[q] = T(0);
       if constexpr (VISC) {
         T gv[5] = {T(0), T(0), T(0), T(0), T(0)};
-        const int oa = off[LO - 1], ob = off[LO];
         T ua[3], ub[3], ga[3][3], gb[3][3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -388,16 +434,18 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
           ub[c] = ring[vel[c] * PS + ob];
         }
         const T i2t1 = T(2) * hsel(t1), i2t2 = T(2) * hsel(t2);
-        ga[1][1] = (ring[vel[1] * PS + ta[1]] - ring[vel[1] * PS + ta[0]]) / i2t1;
-        gb[1][1] = (ring[vel[1] * PS + tb[1]] - ring[vel[1] * PS + tb[0]]) / i2t1;
-        ga[1][0] = (ring[vel[0] * PS + ta[1]] - ring[vel[0] * PS + ta[0]]) / i2t1;
-        gb[1][0] = (ring[vel[0] * PS + tb[1]] - ring[vel[0] * PS + tb[0]]) / i2t1;
-        ga[2][2] = (ring[vel[2] * PS + ta[3]] - ring[vel[2] * PS + ta[2]]) / i2t2;
-        gb[2][2] = (ring[vel[2] * PS + tb[3]] - ring[vel[2] * PS + tb[2]]) / i2t2;
-        ga[2][0] = (ring[vel[0] * PS + ta[3]] - ring[vel[0] * PS + ta[2]]) / i2t2;
-        gb[2][0] = (ring[vel[0] * PS + tb[3]] - ring[vel[0] * PS + tb[2]]) / i2t2;
+        const T ri2t1 = r2sel(t1), ri2t2 = r2sel(t2);
+        ga[1][1] = divk(ring[vel[1] * PS + ta[1]] - ring[vel[1] * PS + ta[0]], i2t1, ri2t1);
+        gb[1][1] = divk(ring[vel[1] * PS + tb[1]] - ring[vel[1] * PS + tb[0]], i2t1, ri2t1);
+        ga[1][0] = divk(ring[vel[0] * PS + ta[1]] - ring[vel[0] * PS + ta[0]], i2t1, ri2t1);
+        gb[1][0] = divk(ring[vel[0] * PS + tb[1]] - ring[vel[0] * PS + tb[0]], i2t1, ri2t1);
+        ga[2][2] = divk(ring[vel[2] * PS + ta[3]] - ring[vel[2] * PS + ta[2]], i2t2, ri2t2);
+        gb[2][2] = divk(ring[vel[2] * PS + tb[3]] - ring[vel[2] * PS + tb[2]], i2t2, ri2t2);
+        ga[2][0] = divk(ring[vel[0] * PS + ta[3]] - ring[vel[0] * PS + ta[2]], i2t2, ri2t2);
+        gb[2][0] = divk(ring[vel[0] * PS + tb[3]] - ring[vel[0] * PS + tb[2]], i2t2, ri2t2);
         viscous_flux<T, 0>(ring[oa], ring[ob], ua, ub, ring[5 * PS + oa],
-                           ring[5 * PS + ob], ga, gb, hsel(dn), nu, inv_pr, gv);
+                           ring[5 * PS + ob], ga, gb, hsel(dn), rsel(dn), nu,
+                           inv_pr, gv);
         rot(gv, fv);
         flux_bc(SWC_FLUX_DIFFUSIVE, fv, fvs);
       }
@@ -409,7 +457,6 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
       return;
     }
     if constexpr (VISC) {
-      const int oa = off[LO - 1], ob = off[LO];
       T ua[3], ub[3], ga[3][3], gb[3][3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -417,18 +464,20 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
         ub[c] = ring[vel[c] * PS + ob];
       }
       const T i2t1 = T(2) * hsel(t1), i2t2 = T(2) * hsel(t2);
+      const T ri2t1 = r2sel(t1), ri2t2 = r2sel(t2);
       // Along t1: components t1 (rotated 1) and n (rotated 0).
-      ga[1][1] = (ring[vel[1] * PS + ta[1]] - ring[vel[1] * PS + ta[0]]) / i2t1;
-      gb[1][1] = (ring[vel[1] * PS + tb[1]] - ring[vel[1] * PS + tb[0]]) / i2t1;
-      ga[1][0] = (ring[vel[0] * PS + ta[1]] - ring[vel[0] * PS + ta[0]]) / i2t1;
-      gb[1][0] = (ring[vel[0] * PS + tb[1]] - ring[vel[0] * PS + tb[0]]) / i2t1;
+      ga[1][1] = divk(ring[vel[1] * PS + ta[1]] - ring[vel[1] * PS + ta[0]], i2t1, ri2t1);
+      gb[1][1] = divk(ring[vel[1] * PS + tb[1]] - ring[vel[1] * PS + tb[0]], i2t1, ri2t1);
+      ga[1][0] = divk(ring[vel[0] * PS + ta[1]] - ring[vel[0] * PS + ta[0]], i2t1, ri2t1);
+      gb[1][0] = divk(ring[vel[0] * PS + tb[1]] - ring[vel[0] * PS + tb[0]], i2t1, ri2t1);
       // Along t2: components t2 (rotated 2) and n.
-      ga[2][2] = (ring[vel[2] * PS + ta[3]] - ring[vel[2] * PS + ta[2]]) / i2t2;
-      gb[2][2] = (ring[vel[2] * PS + tb[3]] - ring[vel[2] * PS + tb[2]]) / i2t2;
-      ga[2][0] = (ring[vel[0] * PS + ta[3]] - ring[vel[0] * PS + ta[2]]) / i2t2;
-      gb[2][0] = (ring[vel[0] * PS + tb[3]] - ring[vel[0] * PS + tb[2]]) / i2t2;
+      ga[2][2] = divk(ring[vel[2] * PS + ta[3]] - ring[vel[2] * PS + ta[2]], i2t2, ri2t2);
+      gb[2][2] = divk(ring[vel[2] * PS + tb[3]] - ring[vel[2] * PS + tb[2]], i2t2, ri2t2);
+      ga[2][0] = divk(ring[vel[0] * PS + ta[3]] - ring[vel[0] * PS + ta[2]], i2t2, ri2t2);
+      gb[2][0] = divk(ring[vel[0] * PS + tb[3]] - ring[vel[0] * PS + tb[2]], i2t2, ri2t2);
       viscous_flux<T, 0>(ring[oa], ring[ob], ua, ub, ring[5 * PS + oa],
-                         ring[5 * PS + ob], ga, gb, hsel(dn), nu, inv_pr, g);
+                         ring[5 * PS + ob], ga, gb, hsel(dn), rsel(dn), nu,
+                         inv_pr, g);
     }
     rot(g, f);
 #pragma unroll
@@ -439,7 +488,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
   // Face of kind `kind` (0 = x-face at row fxx, 1 = y-face at column fyy,
   // 2 = z-face above plane zc) into the flux buffers.
   auto do_face = [&](int kind, int zc, int fxx, int fyy) {
-    int off[NW], ta[4], tb[4];
+    int off[NOFF], ta[4], tb[4];
     T pe;
     T f[NF];
     // Grid-boundary side and face-plane index of this face (EXT only). The
@@ -459,12 +508,12 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
     if (kind == 2) {
       const int pos = (HR + fxx) * PW + HR + fyy;
 #pragma unroll
-      for (int k = 0; k < NW; ++k) off[k] = slot_of(zc + 1 - LO + k) * SL + pos;
+      for (int k = 0; k < CW; ++k) off[k] = slot_of(zc + 1 - CL + k) * SL + pos;
       const int oa = slot_of(zc) * SL + pos, ob = slot_of(zc + 1) * SL + pos;
       ta[0] = oa - PW; ta[1] = oa + PW; ta[2] = oa - 1; ta[3] = oa + 1;
       tb[0] = ob - PW; tb[1] = ob + PW; tb[2] = ob - 1; tb[3] = ob + 1;
       pe = pe_at(x0 + fxx + h, y0 + fyy + h, zc + 1 + h);
-      face(2, off, ta, tb, pe, bside, pidx, f);
+      face(2, off, oa, ob, ta, tb, pe, bside, pidx, f);
 #pragma unroll
       for (int v = 0; v < NF; ++v) fz[(v * TX + fxx) * TY + fyy] = f[v];
     } else {
@@ -480,7 +529,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
       ta[0] = oa - s1; ta[1] = oa + s1; ta[2] = oa + dm; ta[3] = oa + dp;
       tb[0] = ob - s1; tb[1] = ob + s1; tb[2] = ob + dm; tb[3] = ob + dp;
       pe = pe_at(x0 + fxx + h, y0 + fyy + h, zc + h);
-      face(kind, off, ta, tb, pe, bside, pidx, f);
+      face(kind, off, oa, ob, ta, tb, pe, bside, pidx, f);
       if (kind == 0) {
 #pragma unroll
         for (int v = 0; v < NF; ++v) fx[(v * (TX + 1) + fxx) * TY + fyy] = f[v];
@@ -511,19 +560,28 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
   const int xa_c = x0 + tx + h, ya_c = y0 + ty + h;
 
   // Per plane every owner computes three faces of its cell (z above, y and
-  // x below); the last TY + TX threads also compute the tile's high x-row
-  // and high y-column faces; owners of the last interior cell of a partial
-  // tile add the face beyond it.
+  // x below); TY + TX threads also compute the tile's high x-row and high
+  // y-column faces; owners of the last interior cell of a partial tile add
+  // the face beyond it. The boundary block starts at a warp that moves on
+  // from plane to plane (and from tile to tile), so its extra pass falls on
+  // every SM sub-partition in turn instead of always on the last warp's.
   static_assert(TY + TX <= NT, "boundary faces need TY + TX threads");
-  const int wb = tid - (NT - (TY + TX));
-  int nj = own ? 3 : 0;
+  static_assert(NT % 32 == 0, "whole warps");
+  constexpr int NWARP = NT / 32;
+  const int tile_rot = x0 / TX + y0 / TY;
+  const int nj = own ? 3 : 0;
   int bkind = -1, bx = 0, by = 0;
-  if (wb >= 0) {
-    if (wb < TY) { bkind = 0; bx = TX; by = wb; }
-    else { bkind = 1; bx = wb - TY; by = TY; }
-    if (bkind == 0 && !(x0 + TX <= a.nx && y0 + by < a.ny)) bkind = -1;
-    if (bkind == 1 && !(y0 + TY <= a.ny && x0 + bx < a.nx)) bkind = -1;
-  }
+  auto boundary_faces = [&](int zc) {
+    int wb = tid - ((zc - z0 + tile_rot) % NWARP) * 32;
+    if (wb < 0) wb += NT;
+    bkind = -1;
+    if (wb < TY + TX) {
+      if (wb < TY) { bkind = 0; bx = TX; by = wb; }
+      else { bkind = 1; bx = wb - TY; by = TY; }
+      if (bkind == 0 && !(x0 + TX <= a.nx && y0 + by < a.ny)) bkind = -1;
+      if (bkind == 1 && !(y0 + TY <= a.ny && x0 + bx < a.nx)) bkind = -1;
+    }
+  };
   const bool ex_x = own && (x0 + tx + 1 == a.nx) && (tx + 1 < TX);
   const bool ex_y = own && (y0 + ty + 1 == a.ny) && (ty + 1 < TY);
 
@@ -537,6 +595,19 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
     if (zc + 1 < z1) issue_plane(zc + ZHI + 1);
 
     const bool pre = zc < z0;  // only the z-face below the segment
+    if (pre && own) {
+      // Upper-face value of cell z0-1: the lower state of the segment's
+      // first z face.
+      const int pos = (HR + tx) * PW + HR + ty;
+      int off[CW];
+#pragma unroll
+      for (int k = 0; k < CW; ++k) off[k] = slot_of(zc - CL + k) * SL + pos;
+      const int vel[3] = {3, 1, 2};
+      Prim<T> lf;
+      T phlf[NSA], pdlf;
+      recon_all(std::true_type{}, off, vel, lf, zq, phlf, zph, pdlf, zpd);
+    }
+    if (!pre) boundary_faces(zc);
     const int ntot = pre ? (own ? 1 : 0) : nj + (bkind >= 0) + ex_x + ex_y;
     for (int j = 0; j < ntot; ++j) {
       int kind, fxx, fyy;
@@ -593,11 +664,11 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
       for (int v = 0; v < NF; ++v) {
         const T fhi = fz[(v * TX + tx) * TY + ty];
         T rhs = v < 5 ? src[v] : T(0);
-        rhs = rhs - (fx[(v * (TX + 1) + tx + 1) * TY + ty] -
-                     fx[(v * (TX + 1) + tx) * TY + ty]) / dx;
-        rhs = rhs - (fy[(v * TX + tx) * (TY + 1) + ty + 1] -
-                     fy[(v * TX + tx) * (TY + 1) + ty]) / dy;
-        rhs = rhs - (fhi - flo[v]) / dz;
+        rhs = rhs - divk((fx[(v * (TX + 1) + tx + 1) * TY + ty] -
+                     fx[(v * (TX + 1) + tx) * TY + ty]), dx, rdx);
+        rhs = rhs - divk((fy[(v * TX + tx) * (TY + 1) + ty + 1] -
+                     fy[(v * TX + tx) * (TY + 1) + ty]), dy, rdy);
+        rhs = rhs - divk(fhi - flo[v], dz, rdz);
         flo[v] = fhi;
         T r;
         if (a.mode == SWC_OUT_RHS) {
