@@ -29,13 +29,19 @@ namespace {
 // Reverse of the pieces of one face flux.
 // ---------------------------------------------------------------------------
 
-// Reverse of reconstruct_cell<0> (swc_physics.cuh): both WENO5 face values
-// of the cell v[2] from v[0..4] = v[c-2 .. c+2], which share the smoothness
-// indicators. vb[k] += d right/dv[k] * rb + d left/dv[k] * lb.
-template <typename T>
-__device__ __forceinline__ void weno5_cell_vjp(const T* v, T rb, T lb, T* vb) {
-  // Per stencil r: a_r = sum A[r][k] v[k], b_r = sum Bc[r][k] v[k],
-  // beta_r = 13/12 a_r^2 + 1/4 b_r^2 + eps, candidate q_r = sum Q[r][k] v[k].
+// Reverse of recon_cell<0, O> (swc_physics.cuh) on one or two variables
+// (the lanes of O): both WENO5 face values of the cell v[2] from
+// v[0..4] = v[c-2 .. c+2], which share the smoothness indicators.
+// vb[k] += d right/dv[k] * rb + d left/dv[k] * lb. Per stencil r:
+// a_r = sum A[r][k] v[k], b_r = sum Bc[r][k] v[k],
+// beta_r = 13/12 a_r^2 + 1/4 b_r^2 + eps, candidate q_r = sum Q[r][k] v[k].
+template <class O>
+__device__ __forceinline__ void weno5_cell_vjp_v(const typename O::V* v,
+                                                 typename O::V rb,
+                                                 typename O::V lb,
+                                                 typename O::V* vb) {
+  using S = typename O::S;
+  using V = typename O::V;
   constexpr double A[3][5] = {{0, 0, 1, -2, 1}, {0, 1, -2, 1, 0}, {1, -2, 1, 0, 0}};
   constexpr double Bc[3][5] = {{0, 0, 3, -4, 1}, {0, 1, 0, -1, 0}, {1, -4, 3, 0, 0}};
   constexpr double QR[3][5] = {{0, 0, 1.0 / 3, 5.0 / 6, -1.0 / 6},
@@ -45,52 +51,74 @@ __device__ __forceinline__ void weno5_cell_vjp(const T* v, T rb, T lb, T* vb) {
                                {0, 1.0 / 3, 5.0 / 6, -1.0 / 6, 0},
                                {-1.0 / 6, 5.0 / 6, 1.0 / 3, 0, 0}};
   constexpr double DR[3] = {0.3, 0.6, 0.1}, DL[3] = {0.1, 0.6, 0.3};
-  const T c1312 = T(13.0 / 12.0), eps = T(1e-6);
-  T av[3], bv[3], ib[3], iq[3], qr[3], ql[3];
-  T sr = T(0), sl = T(0), nr = T(0), nl = T(0);
+  // acc + c x with c a nonzero stencil coefficient (c = +-1 as an add).
+  auto term = [](double c, V x, V acc, bool first) -> V {
+    if (first) return c == 1 ? x : O::mul(O::splat(S(c)), x);
+    if (c == 1) return O::add(acc, x);
+    if (c == -1) return O::sub(acc, x);
+    return O::fma(O::splat(S(c)), x, acc);
+  };
+  auto lin = [&](const double* c) -> V {
+    V acc = O::splat(S(0));
+    bool first = true;
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+      if (c[k] != 0) {
+        acc = term(c[k], v[k], acc, first);
+        first = false;
+      }
+    return acc;
+  };
+  const V c1312 = O::splat(S(13.0 / 12.0)), eps = O::splat(S(1e-6));
+  V av[3], bv[3], ib[3], iq[3], qr[3], ql[3];
+  V sr, sl, nr, nl;
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
-    T sa = T(0), sb = T(0), sqr = T(0), sql = T(0);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      if (A[r][k] != 0) sa += T(A[r][k]) * v[k];
-      if (Bc[r][k] != 0) sb += T(Bc[r][k]) * v[k];
-      if (QR[r][k] != 0) sqr += T(QR[r][k]) * v[k];
-      if (QL[r][k] != 0) sql += T(QL[r][k]) * v[k];
+    av[r] = lin(A[r]);
+    bv[r] = lin(Bc[r]);
+    qr[r] = lin(QR[r]);
+    ql[r] = lin(QL[r]);
+    const V be = O::add(O::fma(O::mul(c1312, av[r]), av[r],
+                               O::mul(O::mul(O::splat(S(0.25)), bv[r]), bv[r])),
+                        eps);
+    ib[r] = O::rcp(be);         // 1 / beta_r
+    iq[r] = O::mul(ib[r], ib[r]);  // 1 / beta_r^2
+    const V ar = O::mul(O::splat(S(DR[r])), iq[r]);
+    const V al = O::mul(O::splat(S(DL[r])), iq[r]);
+    if (r == 0) {
+      sr = ar;
+      sl = al;
+      nr = O::mul(ar, qr[r]);
+      nl = O::mul(al, ql[r]);
+    } else {
+      sr = O::add(sr, ar);
+      sl = O::add(sl, al);
+      nr = O::fma(ar, qr[r], nr);
+      nl = O::fma(al, ql[r], nl);
     }
-    av[r] = sa;
-    bv[r] = sb;
-    qr[r] = sqr;
-    ql[r] = sql;
-    const T be = c1312 * sa * sa + T(0.25) * sb * sb + eps;
-    ib[r] = rcp_(be);           // 1 / beta_r
-    iq[r] = ib[r] * ib[r];      // 1 / beta_r^2
-    sr += T(DR[r]) * iq[r];
-    sl += T(DL[r]) * iq[r];
-    nr += T(DR[r]) * iq[r] * sqr;
-    nl += T(DL[r]) * iq[r] * sql;
   }
-  const T isr = rcp_(sr), isl = rcp_(sl);
-  const T outr = nr * isr, outl = nl * isl;
-  const T gr = rb * isr, gl = lb * isl;
+  const V isr = O::rcp(sr), isl = O::rcp(sl);
+  const V outr = O::mul(nr, isr), outl = O::mul(nl, isl);
+  const V gr = O::mul(rb, isr), gl = O::mul(lb, isl);
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
     // alpha_r = D_r / beta_r^2; out = sum alpha q / sum alpha.
-    const T qbr = gr * T(DR[r]) * iq[r];
-    const T qbl = gl * T(DL[r]) * iq[r];
-    const T ibq = gr * T(DR[r]) * (qr[r] - outr) + gl * T(DL[r]) * (ql[r] - outl);
+    const V gdr = O::mul(gr, O::splat(S(DR[r])));
+    const V gdl = O::mul(gl, O::splat(S(DL[r])));
+    const V qbr = O::mul(gdr, iq[r]);
+    const V qbl = O::mul(gdl, iq[r]);
+    const V ibq = O::fma(gdr, O::sub(qr[r], outr),
+                         O::mul(gdl, O::sub(ql[r], outl)));
     // d(1/beta^2)/d beta = -2 / beta^3
-    const T bb = T(-2) * ibq * iq[r] * ib[r];
-    const T ca = bb * T(2) * c1312 * av[r];
-    const T cb = bb * T(0.5) * bv[r];
+    const V bb = O::mul(O::mul(O::mul(O::splat(S(-2)), ibq), iq[r]), ib[r]);
+    const V ca = O::mul(O::mul(bb, O::splat(S(2.0 * 13.0 / 12.0))), av[r]);
+    const V cb = O::mul(O::mul(bb, O::splat(S(0.5))), bv[r]);
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
-      T t = T(0);
-      if (QR[r][k] != 0) t += qbr * T(QR[r][k]);
-      if (QL[r][k] != 0) t += qbl * T(QL[r][k]);
-      if (A[r][k] != 0) t += ca * T(A[r][k]);
-      if (Bc[r][k] != 0) t += cb * T(Bc[r][k]);
-      vb[k] += t;
+      if (QR[r][k] != 0) vb[k] = O::fma(O::splat(S(QR[r][k])), qbr, vb[k]);
+      if (QL[r][k] != 0) vb[k] = O::fma(O::splat(S(QL[r][k])), qbl, vb[k]);
+      if (A[r][k] != 0) vb[k] = term(A[r][k], ca, vb[k], false);
+      if (Bc[r][k] != 0) vb[k] = term(Bc[r][k], cb, vb[k], false);
     }
   }
 }
@@ -526,16 +554,20 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
 #pragma unroll
   for (int k = 0; k < 7; ++k)
     P[k] = static_cast<const T*>(D == 1 ? a.primT[k] : a.prim[k]);
-  // Rotated primitive of cell j (normal index with halo = j + h).
-  auto load = [&](int j, T* q) {
+  // The 7 rotated primitives (rho, u_n, u_t1, u_t2, e, p, h) are held as
+  // the pairs (rho, e), (u_n, u_t1), (u_t2, p) and h alone, the grouping of
+  // the forward stage's reconstruction: each pair is one two-lane
+  // instruction stream (Two<T>), h a one-lane one (One<T>).
+  using O2 = Two<T>;
+  using O1 = One<T>;
+  using V2 = typename O2::V;
+  // Rotated primitives of cell j (normal index with halo = j + h).
+  auto load = [&](int j, V2* q, T& qh) {
     const long long o = base + (long long)(j + h) * st;
-    q[0] = P[0][o];
-    q[1] = P[vel[0]][o];
-    q[2] = P[vel[1]][o];
-    q[3] = P[vel[2]][o];
-    q[4] = P[4][o];
-    q[5] = P[5][o];
-    q[6] = P[6][o];
+    q[0] = O2::mk(P[0][o], P[4][o]);
+    q[1] = O2::mk(P[vel[0]][o], P[vel[1]][o]);
+    q[2] = O2::mk(P[vel[2]][o], P[5][o]);
+    qh = P[6][o];
   };
   auto lam_at = [&](int j, T* lv) {
     if (j < 0 || j >= n) {
@@ -547,15 +579,15 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
 #pragma unroll
     for (int v = 0; v < 5; ++v) lv[v] = static_cast<const T*>(LAM[v])[o];
   };
-  auto flush = [&](int j, const T* b) {
+  auto flush = [&](int j, const V2* b, T bh) {
     const long long o = base + (long long)(j + h) * st;
-    atomicAdd(static_cast<T*>(PBAR[0]) + o, b[0]);
-    atomicAdd(static_cast<T*>(PBAR[vel[0]]) + o, b[1]);
-    atomicAdd(static_cast<T*>(PBAR[vel[1]]) + o, b[2]);
-    atomicAdd(static_cast<T*>(PBAR[vel[2]]) + o, b[3]);
-    atomicAdd(static_cast<T*>(PBAR[4]) + o, b[4]);
-    atomicAdd(static_cast<T*>(PBAR[5]) + o, b[5]);
-    atomicAdd(static_cast<T*>(PBAR[6]) + o, b[6]);
+    atomicAdd(static_cast<T*>(PBAR[0]) + o, b[0].x);
+    atomicAdd(static_cast<T*>(PBAR[vel[0]]) + o, b[1].x);
+    atomicAdd(static_cast<T*>(PBAR[vel[1]]) + o, b[1].y);
+    atomicAdd(static_cast<T*>(PBAR[vel[2]]) + o, b[2].x);
+    atomicAdd(static_cast<T*>(PBAR[4]) + o, b[0].y);
+    atomicAdd(static_cast<T*>(PBAR[5]) + o, b[2].y);
+    atomicAdd(static_cast<T*>(PBAR[6]) + o, bh);
   };
   // Window at face i (between cells i-1 and i): primitives sw[k] of cells
   // i-3+k (k = 0..5) and cotangents ab[k] of cells i-3+k (k = 0..4). Step i
@@ -565,29 +597,31 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
   // (face i-1's, carried, and face i's). A cell whose two faces belong to two
   // threads is reversed by both, each with its own face's cotangent (the
   // reverse is linear in them). Cells leave the window complete.
-  T sw[6][7], ab[5][7];
+  V2 sw[6][3], ab[5][3];
+  T swh[6], abh[5];
+  const V2 z2 = O2::splat(T(0));
 #pragma unroll
   for (int k = 0; k < 5; ++k) {
 #pragma unroll
-    for (int v = 0; v < 7; ++v) ab[k][v] = T(0);
+    for (int v = 0; v < 3; ++v) ab[k][v] = z2;
+    abh[k] = T(0);
   }
-  T qn[7], cl[7];  // right value of cell i-1; cotangent of its left value
+  // Right value of cell i-1; cotangent of its left value.
+  V2 qn[3] = {z2, z2, z2}, cl[3] = {z2, z2, z2};
+  T qnh = T(0), clh = T(0);
   T la[5], lb[5];
-#pragma unroll
-  for (int v = 0; v < 7; ++v) {
-    qn[v] = T(0);
-    cl[v] = T(0);
-  }
   if (active) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) load(i0 - 3 + k, sw[k]);
+    for (int k = 0; k < 5; ++k) load(i0 - 3 + k, sw[k], swh[k]);
 #pragma unroll
-    for (int v = 0; v < 7; ++v) {
-      const T s5[5] = {sw[0][v], sw[1][v], sw[2][v], sw[3][v], sw[4][v]};
-      T lv, rv;
-      reconstruct_cell<0>(s5, 0, lv, rv);
-      qn[v] = rv;
+    for (int v = 0; v < 3; ++v) {
+      const V2 s5[5] = {sw[0][v], sw[1][v], sw[2][v], sw[3][v], sw[4][v]};
+      V2 lv;
+      recon_cell<0, O2>(s5, 0, lv, qn[v]);
     }
+    const T s5[5] = {swh[0], swh[1], swh[2], swh[3], swh[4]};
+    T lv;
+    recon_cell<0, O1>(s5, 0, lv, qnh);
   }
   lam_at(active ? i0 - 1 : -1, la);
   const T scale = T(a.beta) / hd;
@@ -620,7 +654,7 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
   if (a.visc && active) tang(base + (long long)(i0 - 1 + h) * st, g4a);
   T nub = T(0);
   for (int i = i0; i < i1; ++i) {
-    load(i + 2, sw[5]);
+    load(i + 2, sw[5], swh[5]);
     lam_at(i, lb);
     T fb[5];
 #pragma unroll
@@ -633,17 +667,22 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
     fr[3] = fb[1 + (D == 2 ? 1 : 2)];
     fr[4] = fb[4];
     // Forward: cell i from cells i-2 .. i+2; face i's states.
-    T lv[7], rn[7];
+    V2 lv[3], rn[3];
+    T lvh, rnh;
 #pragma unroll
-    for (int v = 0; v < 7; ++v) {
-      const T s5[5] = {sw[1][v], sw[2][v], sw[3][v], sw[4][v], sw[5][v]};
-      reconstruct_cell<0>(s5, 0, lv[v], rn[v]);
+    for (int v = 0; v < 3; ++v) {
+      const V2 s5[5] = {sw[1][v], sw[2][v], sw[3][v], sw[4][v], sw[5][v]};
+      recon_cell<0, O2>(s5, 0, lv[v], rn[v]);
+    }
+    {
+      const T s5[5] = {swh[1], swh[2], swh[3], swh[4], swh[5]};
+      recon_cell<0, O1>(s5, 0, lvh, rnh);
     }
     Prim<T> ql, qr;
-    ql.r = qn[0]; ql.u[0] = qn[1]; ql.u[1] = qn[2]; ql.u[2] = qn[3];
-    ql.e = qn[4]; ql.p = qn[5]; ql.h = qn[6];
-    qr.r = lv[0]; qr.u[0] = lv[1]; qr.u[1] = lv[2]; qr.u[2] = lv[3];
-    qr.e = lv[4]; qr.p = lv[5]; qr.h = lv[6];
+    ql.r = qn[0].x; ql.u[0] = qn[1].x; ql.u[1] = qn[1].y; ql.u[2] = qn[2].x;
+    ql.e = qn[0].y; ql.p = qn[2].y; ql.h = qnh;
+    qr.r = lv[0].x; qr.u[0] = lv[1].x; qr.u[1] = lv[1].y; qr.u[2] = lv[2].x;
+    qr.e = lv[0].y; qr.p = lv[2].y; qr.h = lvh;
     int xa, ya, za;  // face cell b = i (pe at the face index)
     {
       const int jb = i + h;
@@ -658,27 +697,29 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
     hllc_vjp<T>(ql, qr, pe, fr, lbar, rbar);
     if (a.visc) {
       // Cells a = i-1 (window 2) and b = i (window 3).
-      const T* ca = sw[2];
-      const T* cb = sw[3];
+      // Cell a: rho, u, p (rotated frame) from the pairs.
+      const T ra_ = sw[2][0].x, rb_ = sw[3][0].x;
+      const T pa_ = sw[2][2].y, pb_ = sw[3][2].y;
       const long long ob = base + (long long)(i + h) * st;
       T g4b[4];
       tang(ob, g4b);
       T rab = T(0), rbb = T(0), pab = T(0), pbb = T(0);
       T uab[3] = {T(0), T(0), T(0)}, ubb[3] = {T(0), T(0), T(0)};
       T gab[4] = {T(0), T(0), T(0), T(0)}, gbb[4] = {T(0), T(0), T(0), T(0)};
-      const T ua[3] = {ca[1], ca[2], ca[3]}, ub[3] = {cb[1], cb[2], cb[3]};
-      nub += viscous_vjp<T>(ca[0], cb[0], ua, ub, ca[5], cb[5], g4a, g4b, hd,
-                            nu, inv_pr, fr, rab, rbb, uab, ubb, pab, pbb, gab,
-                            gbb);
-      ab[2][0] += rab;
-      ab[3][0] += rbb;
-      ab[2][5] += pab;
-      ab[3][5] += pbb;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        ab[2][1 + c] += uab[c];
-        ab[3][1 + c] += ubb[c];
-      }
+      const T ua[3] = {sw[2][1].x, sw[2][1].y, sw[2][2].x};
+      const T ub[3] = {sw[3][1].x, sw[3][1].y, sw[3][2].x};
+      nub += viscous_vjp<T>(ra_, rb_, ua, ub, pa_, pb_, g4a, g4b, hd, nu,
+                            inv_pr, fr, rab, rbb, uab, ubb, pab, pbb, gab, gbb);
+      ab[2][0].x += rab;
+      ab[3][0].x += rbb;
+      ab[2][2].y += pab;
+      ab[3][2].y += pbb;
+      ab[2][1].x += uab[0];
+      ab[3][1].x += ubb[0];
+      ab[2][1].y += uab[1];
+      ab[3][1].y += ubb[1];
+      ab[2][2].x += uab[2];
+      ab[3][2].x += ubb[2];
       // Cell i-1's tangential cotangent is complete (faces i-1 and i).
 #pragma unroll
       for (int c = 0; c < 4; ++c) gba[c] += gab[c];
@@ -691,52 +732,71 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
     }
     // Reverse of cell i-1's reconstruction (cells i-3 .. i+1).
     {
-      const T cr[7] = {lbar.r, lbar.u[0], lbar.u[1], lbar.u[2], lbar.e, lbar.p, lbar.h};
+      const V2 cr[3] = {O2::mk(lbar.r, lbar.e), O2::mk(lbar.u[0], lbar.u[1]),
+                        O2::mk(lbar.u[2], lbar.p)};
 #pragma unroll
-      for (int v = 0; v < 7; ++v) {
-        const T s5[5] = {sw[0][v], sw[1][v], sw[2][v], sw[3][v], sw[4][v]};
-        T sb[5] = {T(0), T(0), T(0), T(0), T(0)};
-        weno5_cell_vjp<T>(s5, cr[v], cl[v], sb);
+      for (int v = 0; v < 3; ++v) {
+        const V2 s5[5] = {sw[0][v], sw[1][v], sw[2][v], sw[3][v], sw[4][v]};
+        V2 acc[5] = {ab[0][v], ab[1][v], ab[2][v], ab[3][v], ab[4][v]};
+        weno5_cell_vjp_v<O2>(s5, cr[v], cl[v], acc);
 #pragma unroll
-        for (int k = 0; k < 5; ++k) ab[k][v] += sb[k];
+        for (int k = 0; k < 5; ++k) ab[k][v] = acc[k];
       }
-      const T cn[7] = {rbar.r, rbar.u[0], rbar.u[1], rbar.u[2], rbar.e, rbar.p, rbar.h};
+      {
+        const T s5[5] = {swh[0], swh[1], swh[2], swh[3], swh[4]};
+        T acc[5] = {abh[0], abh[1], abh[2], abh[3], abh[4]};
+        weno5_cell_vjp_v<O1>(s5, lbar.h, clh, acc);
 #pragma unroll
-      for (int v = 0; v < 7; ++v) {
-        cl[v] = cn[v];
-        qn[v] = rn[v];
+        for (int k = 0; k < 5; ++k) abh[k] = acc[k];
       }
+      cl[0] = O2::mk(rbar.r, rbar.e);
+      cl[1] = O2::mk(rbar.u[0], rbar.u[1]);
+      cl[2] = O2::mk(rbar.u[2], rbar.p);
+      clh = rbar.h;
+#pragma unroll
+      for (int v = 0; v < 3; ++v) qn[v] = rn[v];
+      qnh = rnh;
     }
     // Cell i-3 is complete: flush it and slide.
-    flush(i - 3, ab[0]);
+    flush(i - 3, ab[0], abh[0]);
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
 #pragma unroll
-      for (int v = 0; v < 7; ++v) sw[k][v] = sw[k + 1][v];
+      for (int v = 0; v < 3; ++v) sw[k][v] = sw[k + 1][v];
+      swh[k] = swh[k + 1];
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
 #pragma unroll
-      for (int v = 0; v < 7; ++v) ab[k][v] = ab[k + 1][v];
+      for (int v = 0; v < 3; ++v) ab[k][v] = ab[k + 1][v];
+      abh[k] = abh[k + 1];
     }
 #pragma unroll
-    for (int v = 0; v < 7; ++v) ab[4][v] = T(0);
+    for (int v = 0; v < 3; ++v) ab[4][v] = z2;
+    abh[4] = T(0);
 #pragma unroll
     for (int v = 0; v < 5; ++v) la[v] = lb[v];
   }
   if (active) {
     // Cell i1-1: only its left face (face i1-1) belongs to this thread.
 #pragma unroll
-    for (int v = 0; v < 7; ++v) {
-      const T s5[5] = {sw[0][v], sw[1][v], sw[2][v], sw[3][v], sw[4][v]};
-      T sb[5] = {T(0), T(0), T(0), T(0), T(0)};
-      weno5_cell_vjp<T>(s5, T(0), cl[v], sb);
+    for (int v = 0; v < 3; ++v) {
+      const V2 s5[5] = {sw[0][v], sw[1][v], sw[2][v], sw[3][v], sw[4][v]};
+      V2 acc[5] = {ab[0][v], ab[1][v], ab[2][v], ab[3][v], ab[4][v]};
+      weno5_cell_vjp_v<O2>(s5, z2, cl[v], acc);
 #pragma unroll
-      for (int k = 0; k < 5; ++k) ab[k][v] += sb[k];
+      for (int k = 0; k < 5; ++k) ab[k][v] = acc[k];
+    }
+    {
+      const T s5[5] = {swh[0], swh[1], swh[2], swh[3], swh[4]};
+      T acc[5] = {abh[0], abh[1], abh[2], abh[3], abh[4]};
+      weno5_cell_vjp_v<O1>(s5, T(0), clh, acc);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) abh[k] = acc[k];
     }
     // Cells i1-3 .. i1+1 may still hold contributions.
 #pragma unroll
-    for (int k = 0; k < 5; ++k) flush(i1 - 3 + k, ab[k]);
+    for (int k = 0; k < 5; ++k) flush(i1 - 3 + k, ab[k], abh[k]);
     if (a.visc) tang_flush(base + (long long)(i1 - 1 + h) * st, gba);
   }
   if (a.visc && a.nu_bar) {
