@@ -655,6 +655,33 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
   T nub = T(0);
   for (int i = i0; i < i1; ++i) {
     load(i + 2, sw[5], swh[5]);
+    if (i + 1 < i1) {
+      // Start the next step's global reads (window cell i+3, lambda of cell
+      // i+1, tangential neighbours of cell i+1) towards L1: the flux
+      // reverse of this step hides their latency.
+      const long long o3 = base + (long long)(i + 3 + h) * st;
+      prefetch_l1(P[0] + o3);
+      prefetch_l1(P[4] + o3);
+      prefetch_l1(P[5] + o3);
+      prefetch_l1(P[6] + o3);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) prefetch_l1(P[vel[k]] + o3);
+      const long long o1 = base + (long long)(i + 1 + h) * st;
+      if (i + 1 < n) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) prefetch_l1(static_cast<const T*>(LAM[v]) + o1);
+      }
+      if (a.visc) {
+        prefetch_l1(P[vel[1]] + o1 + s1);
+        prefetch_l1(P[vel[1]] + o1 - s1);
+        prefetch_l1(P[vel[0]] + o1 + s1);
+        prefetch_l1(P[vel[0]] + o1 - s1);
+        prefetch_l1(P[vel[2]] + o1 + s2);
+        prefetch_l1(P[vel[2]] + o1 - s2);
+        prefetch_l1(P[vel[0]] + o1 + s2);
+        prefetch_l1(P[vel[0]] + o1 - s2);
+      }
+    }
     lam_at(i, lb);
     T fb[5];
 #pragma unroll

@@ -111,6 +111,11 @@ __device__ __forceinline__ void cp_async(T* smem, const T* gmem) {
                  "l"(gmem));
   }
 }
+// Hint that the line holding *p will be read soon (no register is used;
+// callers pass only addresses they will load).
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];\n" ::"l"(p));
+}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::);
 }
