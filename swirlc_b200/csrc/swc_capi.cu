@@ -178,7 +178,7 @@ __global__ void recon_kernel(Geo3 g, int dim, int limiter, const T* v, T* neg,
 #pragma unroll
     for (int k = 0; k < LO + RI; ++k) s[k] = v[o + (k - LO) * st];
     T a, b;
-    reconstruct<S>(s, limiter, a, b);
+    recon_face<S, One<T>>(s, limiter, a, b);
     neg[o] = a;
     pos[o] = b;
   }

@@ -105,79 +105,6 @@ struct Stencil<3> {  // NODE (identity)
   static constexpr int LO = 0, RI = 1;
 };
 
-// WENO5 value on the right face (c+1/2) of cell c from v[c-2..c+2].
-template <typename T>
-__device__ __forceinline__ T weno5_right(T vm2, T vm1, T v0, T vp1, T vp2) {
-  const T c1312 = T(13.0 / 12.0), q = T(0.25), eps = T(1e-6);
-  T a = v0 - T(2) * vp1 + vp2, b = T(3) * v0 - T(4) * vp1 + vp2;
-  T b0 = c1312 * a * a + q * b * b;
-  a = vm1 - T(2) * v0 + vp1;
-  b = vm1 - vp1;
-  T b1 = c1312 * a * a + q * b * b;
-  a = vm2 - T(2) * vm1 + v0;
-  b = vm2 - T(4) * vm1 + T(3) * v0;
-  T b2 = c1312 * a * a + q * b * b;
-  b0 += eps;
-  b1 += eps;
-  b2 += eps;
-  T a0 = T(0.3) * rcp_(b0 * b0);
-  T a1 = T(0.6) * rcp_(b1 * b1);
-  T a2 = T(0.1) * rcp_(b2 * b2);
-  T q0 = T(1.0 / 3.0) * v0 + T(5.0 / 6.0) * vp1 - T(1.0 / 6.0) * vp2;
-  T q1 = T(-1.0 / 6.0) * vm1 + T(5.0 / 6.0) * v0 + T(1.0 / 3.0) * vp1;
-  T q2 = T(1.0 / 3.0) * vm2 - T(7.0 / 6.0) * vm1 + T(11.0 / 6.0) * v0;
-  return (a0 * q0 + a1 * q1 + a2 * q2) * rcp_(a0 + a1 + a2);
-}
-
-// WENO5 value on the left face (c-1/2) of cell c from v[c-2..c+2].
-template <typename T>
-__device__ __forceinline__ T weno5_left(T vm2, T vm1, T v0, T vp1, T vp2) {
-  const T c1312 = T(13.0 / 12.0), q = T(0.25), eps = T(1e-6);
-  T a = v0 - T(2) * vp1 + vp2, b = T(3) * v0 - T(4) * vp1 + vp2;
-  T b0 = c1312 * a * a + q * b * b;
-  a = vm1 - T(2) * v0 + vp1;
-  b = vm1 - vp1;
-  T b1 = c1312 * a * a + q * b * b;
-  a = vm2 - T(2) * vm1 + v0;
-  b = vm2 - T(4) * vm1 + T(3) * v0;
-  T b2 = c1312 * a * a + q * b * b;
-  b0 += eps;
-  b1 += eps;
-  b2 += eps;
-  T a0 = T(0.1) * rcp_(b0 * b0);
-  T a1 = T(0.6) * rcp_(b1 * b1);
-  T a2 = T(0.3) * rcp_(b2 * b2);
-  T q0 = T(11.0 / 6.0) * v0 - T(7.0 / 6.0) * vp1 + T(1.0 / 3.0) * vp2;
-  T q1 = T(1.0 / 3.0) * vm1 + T(5.0 / 6.0) * v0 - T(1.0 / 6.0) * vp1;
-  T q2 = T(-1.0 / 6.0) * vm2 + T(5.0 / 6.0) * vm1 + T(1.0 / 3.0) * v0;
-  return (a0 * q0 + a1 * q1 + a2 * q2) * rcp_(a0 + a1 + a2);
-}
-
-// WENO3 (k = 2) right / left face values of cell c from v[c-1..c+1], with
-// d = (2/3, 1/3) and candidates c[-1..1] = (3/2,-1/2), (1/2,1/2), (-1/2,3/2).
-template <typename T>
-__device__ __forceinline__ T weno3_right(T vm1, T v0, T vp1) {
-  const T eps = T(1e-6);
-  T b0 = (vp1 - v0) * (vp1 - v0) + eps;
-  T b1 = (v0 - vm1) * (v0 - vm1) + eps;
-  T a0 = T(2.0 / 3.0) * rcp_(b0 * b0);
-  T a1 = T(1.0 / 3.0) * rcp_(b1 * b1);
-  T q0 = T(0.5) * v0 + T(0.5) * vp1;
-  T q1 = T(-0.5) * vm1 + T(1.5) * v0;
-  return (a0 * q0 + a1 * q1) * rcp_(a0 + a1);
-}
-template <typename T>
-__device__ __forceinline__ T weno3_left(T vm1, T v0, T vp1) {
-  const T eps = T(1e-6);
-  T b0 = (vp1 - v0) * (vp1 - v0) + eps;
-  T b1 = (v0 - vm1) * (v0 - vm1) + eps;
-  T a0 = T(1.0 / 3.0) * rcp_(b0 * b0);
-  T a1 = T(2.0 / 3.0) * rcp_(b1 * b1);
-  T q0 = T(1.5) * v0 - T(0.5) * vp1;
-  T q1 = T(0.5) * vm1 + T(0.5) * v0;
-  return (a0 * q0 + a1 * q1) * rcp_(a0 + a1);
-}
-
 // MUSCL slope of cell c: phi(r) * dp with r = dnn(dm, dp).
 template <typename T>
 __device__ __forceinline__ T muscl_slope(T vm1, T v0, T vp1, int limiter) {
@@ -227,64 +154,6 @@ template <>
 struct CellStencil<3> {
   static constexpr int CL = 0, CR = 1;
 };
-
-template <int SCHEME, typename T>
-__device__ __forceinline__ void reconstruct_cell(const T* s, int limiter,
-                                                 T& left, T& right) {
-  if constexpr (SCHEME == 0) {
-    const T vm2 = s[0], vm1 = s[1], v0 = s[2], vp1 = s[3], vp2 = s[4];
-    const T c1312 = T(13.0 / 12.0), q = T(0.25), eps = T(1e-6);
-    T a = v0 - T(2) * vp1 + vp2, b = T(3) * v0 - T(4) * vp1 + vp2;
-    T b0 = c1312 * a * a + q * b * b;
-    a = vm1 - T(2) * v0 + vp1;
-    b = vm1 - vp1;
-    T b1 = c1312 * a * a + q * b * b;
-    a = vm2 - T(2) * vm1 + v0;
-    b = vm2 - T(4) * vm1 + T(3) * v0;
-    T b2 = c1312 * a * a + q * b * b;
-    b0 += eps;
-    b1 += eps;
-    b2 += eps;
-    const T i0 = rcp_(b0 * b0), i1 = rcp_(b1 * b1), i2 = rcp_(b2 * b2);
-    {  // right face: d = (0.3, 0.6, 0.1)
-      const T a0 = T(0.3) * i0, a1 = T(0.6) * i1, a2 = T(0.1) * i2;
-      const T q0 = T(1.0 / 3.0) * v0 + T(5.0 / 6.0) * vp1 - T(1.0 / 6.0) * vp2;
-      const T q1 = T(-1.0 / 6.0) * vm1 + T(5.0 / 6.0) * v0 + T(1.0 / 3.0) * vp1;
-      const T q2 = T(1.0 / 3.0) * vm2 - T(7.0 / 6.0) * vm1 + T(11.0 / 6.0) * v0;
-      right = (a0 * q0 + a1 * q1 + a2 * q2) * rcp_(a0 + a1 + a2);
-    }
-    {  // left face: d = (0.1, 0.6, 0.3)
-      const T a0 = T(0.1) * i0, a1 = T(0.6) * i1, a2 = T(0.3) * i2;
-      const T q0 = T(11.0 / 6.0) * v0 - T(7.0 / 6.0) * vp1 + T(1.0 / 3.0) * vp2;
-      const T q1 = T(1.0 / 3.0) * vm1 + T(5.0 / 6.0) * v0 - T(1.0 / 6.0) * vp1;
-      const T q2 = T(-1.0 / 6.0) * vm2 + T(5.0 / 6.0) * vm1 + T(1.0 / 3.0) * v0;
-      left = (a0 * q0 + a1 * q1 + a2 * q2) * rcp_(a0 + a1 + a2);
-    }
-  } else if constexpr (SCHEME == 1) {
-    const T vm1 = s[0], v0 = s[1], vp1 = s[2];
-    const T eps = T(1e-6);
-    T b0 = (vp1 - v0) * (vp1 - v0) + eps;
-    T b1 = (v0 - vm1) * (v0 - vm1) + eps;
-    const T i0 = rcp_(b0 * b0), i1 = rcp_(b1 * b1);
-    {
-      const T a0 = T(2.0 / 3.0) * i0, a1 = T(1.0 / 3.0) * i1;
-      right = (a0 * (T(0.5) * v0 + T(0.5) * vp1) +
-               a1 * (T(-0.5) * vm1 + T(1.5) * v0)) * rcp_(a0 + a1);
-    }
-    {
-      const T a0 = T(1.0 / 3.0) * i0, a1 = T(2.0 / 3.0) * i1;
-      left = (a0 * (T(1.5) * v0 - T(0.5) * vp1) +
-              a1 * (T(0.5) * vm1 + T(0.5) * v0)) * rcp_(a0 + a1);
-    }
-  } else if constexpr (SCHEME == 2) {
-    const T sl = muscl_slope(s[0], s[1], s[2], limiter);
-    right = s[1] + T(0.5) * sl;
-    left = s[1] - T(0.5) * sl;
-  } else {
-    left = s[0];
-    right = s[1];
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Lane-generic reconstruction used by the fused stage. Face reconstruction
@@ -537,24 +406,6 @@ __device__ __forceinline__ void recon_cell(const typename O::V* s, int limiter,
   } else {
     left = s[0];
     right = s[1];
-  }
-}
-
-template <int SCHEME, typename T>
-__device__ __forceinline__ void reconstruct(const T* s, int limiter, T& neg,
-                                            T& pos) {
-  if constexpr (SCHEME == 0) {
-    neg = weno5_right(s[0], s[1], s[2], s[3], s[4]);
-    pos = weno5_left(s[1], s[2], s[3], s[4], s[5]);
-  } else if constexpr (SCHEME == 1) {
-    neg = weno3_right(s[0], s[1], s[2]);
-    pos = weno3_left(s[1], s[2], s[3]);
-  } else if constexpr (SCHEME == 2) {
-    neg = s[1] + T(0.5) * muscl_slope(s[0], s[1], s[2], limiter);
-    pos = s[2] - T(0.5) * muscl_slope(s[1], s[2], s[3], limiter);
-  } else {
-    neg = s[0];
-    pos = s[0];
   }
 }
 
