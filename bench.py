@@ -56,17 +56,27 @@ def _peaks():
     return 6650.0, 'fallback'
 
 
-def _traffic_from_profiles():
-  """Per-launch DRAM bytes of the stage kernel from the committed ncu summary."""
+def _profile_figure(key):
+  """A per-cell figure of the stage kernel from the committed ncu summary."""
   path = os.path.join(ROOT, 'profiles', 'stage_kernel_kh256.txt')
   try:
     with open(path) as f:
       for line in f:
-        if line.startswith('traffic_bytes_per_cell_stage:'):
+        if line.startswith(key + ':'):
           return float(line.split(':', 1)[1])
   except OSError:
     pass
   return None
+
+
+def _traffic_from_profiles():
+  """Per-launch DRAM bytes per cell of the stage kernel (ncu)."""
+  return _profile_figure('traffic_bytes_per_cell_stage')
+
+
+# SMs x FP32 lanes per SM of a B200: the FMA-pipe lane rate is this times the
+# SM clock.
+FP32_LANES = 148 * 128
 
 
 class ClockSampler:
@@ -203,6 +213,20 @@ def run_ours(args):
   achieved = tot_bytes / (tot_ms / 1e3) / 1e9
   peak, peak_kind = _peaks()
   traffic_pc = _traffic_from_profiles()
+  # The bound that holds the stage kernel: its FMA-pipe work (FP32 lane
+  # operations per cell and stage, ncu) over the FMA-pipe lane rate at the
+  # SM clock sampled during the timed region.
+  lane_ops = _profile_figure('fp32_lane_ops_per_cell_stage')
+  fp32_pipe = None
+  if lane_ops is not None:
+    mhz = clocks.get('sm_mhz') or 1965.0
+    ach = lane_ops * cells * len(evs) / (tot_ms / 1e3) / 1e12
+    pk = FP32_LANES * mhz * 1e6 / 1e12
+    fp32_pipe = {'achieved': ach, 'peak': pk, 'unit': 'T lane-ops/s',
+                 'frac': ach / pk, 'ops_per_cell_stage': lane_ops,
+                 'note': 'FMA-pipe cycles x 128 lanes per SM (an f32x2 '
+                         'instruction counts its two lanes); the stage '
+                         'kernel is bound here, not by HBM'}
 
   # End-to-end through the public API: host state -> Simulation.step -> host.
   sim = simulation.Simulation(None, cfg)
@@ -258,7 +282,8 @@ def run_ours(args):
                      'peak_source': peak_kind,
                      'traffic': None if traffic_pc is None else traffic_pc * cells,
                      'kernel': 'stage_kernel (3 launches per step, algorithmic '
-                               '40/60/60 B per cell)'},
+                               '40/60/60 B per cell)',
+                     'fp32_pipe': fp32_pipe},
         'cpu_baseline': cpu,
         'e2e': {'value': world * cells * e2e_steps / (e2e_ms / 1e3), 'unit': UNIT,
                 'h2d_bytes_per_step': state_bytes,
