@@ -13,7 +13,11 @@
 // centre plane into shared memory, computes the z-face above each column in
 // registers (the face below is carried from the previous step), then forms
 // the divergence and the stage update of the centre plane. Each face flux is
-// computed exactly once per CTA.
+// computed exactly once per CTA. x and y faces reconstruct both face states
+// from the face's stencil; z faces take them from cell-centred
+// reconstructions of the column's cells, one per cell, whose upper-face
+// value is carried up the column. The primitives are reconstructed two at a
+// time (f32x2 lanes), all with explicitly rounded operations.
 #pragma once
 
 #include <type_traits>
