@@ -971,11 +971,21 @@ __global__ void __launch_bounds__(256) vjp_halo_kernel(const VjpHalo a) {
   const int h = a.h;
   const int nxa = a.nx + 2 * h, nya = a.ny + 2 * h, nza = a.nz + 2 * h;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)nxa * nya * nza) return;
-  const int ya = (int)(t % nya);
-  const long long r = t / nya;
-  const int xa = (int)(r % nxa);
-  const int za = (int)(r / nxa);
+  const long long cells = (long long)nxa * nya * nza;
+  if (t >= cells) return;
+  int ya, xa, za;
+  if (cells < (1LL << 32)) {  // 32-bit division where the grid fits
+    const unsigned tt = (unsigned)t;
+    const unsigned r = tt / (unsigned)nya;
+    ya = (int)(tt - r * (unsigned)nya);
+    za = (int)(r / (unsigned)nxa);
+    xa = (int)(r - (unsigned)za * (unsigned)nxa);
+  } else {
+    ya = (int)(t % nya);
+    const long long r = t / nya;
+    xa = (int)(r % nxa);
+    za = (int)(r / nxa);
+  }
   const int c[3] = {xa, ya, za};
   const int n[3] = {a.nx, a.ny, a.nz};
   int side[3];

@@ -51,10 +51,26 @@ __device__ __forceinline__ void halo_elem(const A& a, long long t) {
   const long long plane = (long long)na * nb;
   const int n = ext[d] - 2 * a.h;
   {
-    const long long pb = t % plane;
-    const int side = (int)((t / plane) % 2);
-    const int fi = (int)(t / (plane * 2));
-    const int ia = (int)(pb / nb), ib = (int)(pb % nb);
+    // Element t -> (field, side, plane position). 32-bit unsigned division
+    // where the pass fits (a 64-bit division is a long software sequence).
+    long long pb;
+    int side, fi, ia, ib;
+    if (plane * 2 * a.nf < (1LL << 32)) {
+      const unsigned tt = (unsigned)t, pl = (unsigned)plane;
+      const unsigned q = tt / pl;
+      const unsigned p = tt - q * pl;
+      side = (int)(q & 1u);
+      fi = (int)(q >> 1);
+      ia = (int)(p / (unsigned)nb);
+      ib = (int)(p - (unsigned)ia * (unsigned)nb);
+      pb = p;
+    } else {
+      pb = t % plane;
+      side = (int)((t / plane) % 2);
+      fi = (int)(t / (plane * 2));
+      ia = (int)(pb / nb);
+      ib = (int)(pb % nb);
+    }
     const long long base = ia * stride[ax_a] + ib * stride[ax_b];
     const long long sd = stride[d];
     T* f = static_cast<T*>(a.fld[fi].f);
