@@ -63,10 +63,18 @@ class RunAdjoint:
     self._tmp = None       # stage buffers of steps that keep nothing
     self._u = None         # working state of the recomputed segment
     self._ckpt_pool: List = []  # checkpoint states, reused
+    # Index of the segment whose stage states the last run() left in
+    # self._pool (the final one), or -1: its reverse needs no recompute.
+    self._kept = -1
     if steps:
       self._reserve(steps if self.k == 0 else min(self.k, steps))
       if self.k:
         self._reserve_checkpoints((steps + self.k - 1) // self.k)
+      if self.k and steps > self.k:
+        # Stage buffers of the steps that keep nothing, and the working state
+        # of the segment recompute: allocated here, not inside a run.
+        self._tmp = self._new_buffers()
+        self._u = solver.new_fields(zero=False)
 
   # ------------------------------------------------------------- forward
   def _new_buffers(self):
@@ -112,8 +120,14 @@ class RunAdjoint:
     self.dts = [float(d) for d in dts]
     u = [f.detach().clone() for f in fields]
     self.checkpoints = []
+    self._kept = -1
     if self.k == 0:
       self._reserve(len(self.dts))
+    else:
+      self._reserve(min(self.k, len(self.dts)))
+    # The final segment's stage states stay in the pool: the reverse sweep
+    # starts there, so it needs no recompute of that segment.
+    last_seg = (len(self.dts) - 1) // self.k if self.k and self.dts else -1
     for i, dt in enumerate(self.dts):
       if self.k == 0:
         self._step(u, dt, self._pool[i])
@@ -124,7 +138,11 @@ class RunAdjoint:
         for a, b in zip(self._ckpt_pool[c], u):
           a.copy_(b)
         self.checkpoints.append(self._ckpt_pool[c])
-      self._step(u, dt)
+      if i // self.k == last_seg:
+        self._step(u, dt, self._pool[i - last_seg * self.k])
+      else:
+        self._step(u, dt)
+    self._kept = last_seg
     if self.k == 0:
       self.checkpoints = [None]
     self.s.fill_halos(u)
@@ -179,13 +197,16 @@ class RunAdjoint:
       for c in reversed(range(len(self.checkpoints))):
         first = c * self.k
         last = min(first + self.k, nsteps)
-        if self._u is None:
-          self._u = self.s.new_fields(zero=False)
-        u = self._u
-        for a, b in zip(u, self.checkpoints[c]):
-          a.copy_(b)
-        for i in range(first, last):
-          self._step(u, self.dts[i], self._pool[i - first])
+        if c != self._kept:
+          if self._u is None:
+            self._u = self.s.new_fields(zero=False)
+          u = self._u
+          for a, b in zip(u, self.checkpoints[c]):
+            a.copy_(b)
+          for i in range(first, last):
+            self._step(u, self.dts[i], self._pool[i - first])
+        # The pool now holds segment c; later sweeps recompute everything.
+        self._kept = -1
         for i in reversed(range(first, last)):
           self._reverse_step(self._pool[i - first], self.dts[i], g, gn, g2,
                              g1)
