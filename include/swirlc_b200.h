@@ -266,8 +266,10 @@ int swc_batch_step(const SwcScheme* scheme, int32_t order, int32_t nmembers,
  * cotangent A*lam, which x1 / x2 let the caller fold in. vout must not alias
  * uk, lam, x1 or x2. `scratch` is SWC_VJP_SCRATCH caller buffers of the
  * shape of uk (primitives and their cotangents, and copies transposed to
- * [z][y][x] for the y faces). The reference differentiates this path with
- * TF's GradientTape; this is its discrete adjoint. */
+ * [z][y][x] for the y faces). The first call in a process sets the
+ * kernels' shared-memory limit for its dtype: make it outside stream
+ * capture. The reference differentiates this path with TF's GradientTape;
+ * this is its discrete adjoint. */
 #define SWC_VJP_SCRATCH 33
 int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* scheme,
                      const SwcFieldBC* bcs, const void* const* uk,

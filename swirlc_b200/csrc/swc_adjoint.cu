@@ -432,12 +432,20 @@ constexpr int TT = 32;
 
 // Primitives of every cell (halos included), in both layouts, with their
 // cotangent buffers cleared, and lam transposed.
+// Dynamic shared memory of the transposing kernels: one [TT][TT+1] tile
+// per transposed variable, so a single barrier separates all writers from
+// all readers.
+constexpr int kPrimTiles = 12;  // 7 primitives + 5 lambda fields
+constexpr int kCellTiles = 7;   // 7 primitive cotangents
+template <typename T>
+__device__ __forceinline__ T (*vjp_tiles())[TT][TT + 1] {
+  extern __shared__ __align__(16) unsigned char vjp_smem[];
+  return reinterpret_cast<T(*)[TT][TT + 1]>(vjp_smem);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) vjp_prim_kernel(const VjpArgs a) {
-  // Two tiles: variable v goes through tile v % 2, so one barrier per
-  // variable separates its writers from its readers and from the writers
-  // two variables later.
-  __shared__ T tiles[2][TT][TT + 1];
+  T(*tiles)[TT][TT + 1] = vjp_tiles<T>();
   const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h;
   const int za = blockIdx.z;
   const int y0 = blockIdx.x * TT, x0 = blockIdx.y * TT;
@@ -474,15 +482,17 @@ __global__ void __launch_bounds__(256) vjp_prim_kernel(const VjpArgs a) {
       static_cast<T*>(a.pbar[v])[o] = T(0);
     }
   }
-  // tile[x - x0][y - y0]; the transposed write reads it along x.
+  // tiles[v][x - x0][y - y0]; the transposed write reads them along x.
 #pragma unroll
-  for (int v = 0; v < 12; ++v) {
-    T(*tile)[TT + 1] = tiles[v & 1];
+  for (int v = 0; v < kPrimTiles; ++v) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      tile[ty + 8 * k][tx] = v < 7 ? pr[k][v] : lv[k][v - 7];
-    }
-    __syncthreads();
+    for (int k = 0; k < 4; ++k)
+      tiles[v][ty + 8 * k][tx] = v < 7 ? pr[k][v] : lv[k][v - 7];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int v = 0; v < kPrimTiles; ++v) {
+    T(*tile)[TT + 1] = tiles[v];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int yl = ty + 8 * k;
@@ -840,7 +850,7 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
 // cotangents are read back from the transposed layout through a tile.
 template <typename T>
 __global__ void __launch_bounds__(256) vjp_cell_kernel(const VjpArgs a) {
-  __shared__ T tiles[2][TT][TT + 1];  // as in vjp_prim_kernel
+  T(*tiles)[TT][TT + 1] = vjp_tiles<T>();  // as in vjp_prim_kernel
   const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h;
   const int za = blockIdx.z;
   const int y0 = blockIdx.x * TT, x0 = blockIdx.y * TT;
@@ -867,15 +877,17 @@ __global__ void __launch_bounds__(256) vjp_cell_kernel(const VjpArgs a) {
     for (int v = 0; v < 5; ++v)
       c4[k][v] = in ? static_cast<const T*>(a.uk[v])[o] : T(1);
   }
-  // tile[y - y0][x - x0], written along x, read along y.
+  // tiles[v][y - y0][x - x0], written along x, read along y.
 #pragma unroll
-  for (int v = 0; v < 7; ++v) {
-    T(*tile)[TT + 1] = tiles[v & 1];
+  for (int v = 0; v < kCellTiles; ++v) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) tile[ty + 8 * k][tx] = pbt[k][v];
-    __syncthreads();
+    for (int k = 0; k < 4; ++k) tiles[v][ty + 8 * k][tx] = pbt[k][v];
+  }
+  __syncthreads();
 #pragma unroll
-    for (int k = 0; k < 4; ++k) pbs[k][v] += tile[tx][ty + 8 * k];
+  for (int v = 0; v < kCellTiles; ++v) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) pbs[k][v] += tiles[v][tx][ty + 8 * k];
   }
   T l4[4][5], x14[4][5], x24[4][5];
 #pragma unroll
@@ -1033,7 +1045,22 @@ int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
   const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h, nza = a.nz + 2 * a.h;
   const dim3 tgrid((nya + TT - 1) / TT, (nxa + TT - 1) / TT, nza);
   const dim3 tblock(TT, 8);
-  vjp_prim_kernel<T><<<tgrid, tblock, 0, s>>>(a);
+  const size_t tile_bytes = sizeof(T) * TT * (TT + 1);
+  // Above 48 KB of dynamic shared memory a kernel must opt in: done on the
+  // first call per dtype, which the header asks callers to make outside
+  // stream capture.
+  static bool smem_set = false;
+  if (!smem_set) {
+    if (cudaFuncSetAttribute(vjp_prim_kernel<T>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(kPrimTiles * tile_bytes)) != cudaSuccess ||
+        cudaFuncSetAttribute(vjp_cell_kernel<T>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(kCellTiles * tile_bytes)) != cudaSuccess)
+      return record_error(SWC_ERR_LAUNCH, "stage vjp: shared memory opt-in");
+    smem_set = true;
+  }
+  vjp_prim_kernel<T><<<tgrid, tblock, kPrimTiles * tile_bytes, s>>>(a);
   note_launch();
   const int ft = 128;
   for (int D = 0; D < 3; ++D) {
@@ -1048,7 +1075,7 @@ int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
     else vjp_face_kernel<T, 2><<<blocks, ft, 0, s>>>(a);
     note_launch();
   }
-  vjp_cell_kernel<T><<<tgrid, tblock, 0, s>>>(a);
+  vjp_cell_kernel<T><<<tgrid, tblock, kCellTiles * tile_bytes, s>>>(a);
   note_launch();
   {
     VjpHalo hh;
