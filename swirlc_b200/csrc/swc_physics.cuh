@@ -237,21 +237,27 @@ struct Two<double> {
   }
 };
 
-// WENO5-JS on the cell stencil v[c-2..c+2]: the reciprocals
-// i_r = 1/(eps + beta_r)^2 of the three candidate stencils (shared by both
-// faces of the cell), then the value on the right face (c+1/2, linear
-// weights d = (0.3, 0.6, 0.1)) and on the left face (c-1/2, d mirrored);
-// candidate polynomials of the reference prototype's `weno5`.
+// WENO5-JS on the cell stencil v[c-2..c+2]: alpha_r = d_r / (eps + beta_r)^2
+// with eps = 1e-6, the smoothness indicators
+// beta_r = 13/12 a_r^2 + 1/4 b_r^2 and the candidate polynomials q_r of the
+// reference prototype's `weno5`; the value is sum alpha_r q_r / sum alpha_r.
+// Computed as: B_r = 4 (beta_r + eps) = 13/3 a_r^2 + (b_r^2 + 4 eps) (eps
+// folds into an FMA), i_r = 1/B_r^2 (shared by both faces of the cell), and
+// per face num = sum i_r (d_r q_r), den = sum d_r i_r with d_r folded into
+// the candidates' coefficients. The common factor 1/16 of i_r cancels in
+// num/den, so the weights are the prototype's in exact arithmetic.
+// Right face (c+1/2): d = (0.3, 0.6, 0.1); left face (c-1/2): d mirrored.
 template <class O>
 struct Weno5Inv {
   typename O::V i0, i1, i2;
 };
+// 4 (beta + eps) from the stencil differences a and b.
 template <class O>
-__device__ __forceinline__ typename O::V weno5_beta(typename O::V a,
-                                                    typename O::V b) {
+__device__ __forceinline__ typename O::V weno5_b4(typename O::V a,
+                                                  typename O::V b) {
   using S = typename O::S;
-  return O::fma(O::mul(O::splat(S(13.0 / 12.0)), a), a,
-                O::mul(O::mul(O::splat(S(0.25)), b), b));
+  return O::fma(O::mul(O::splat(S(13.0 / 3.0)), a), a,
+                O::fma(b, b, O::splat(S(4e-6))));
 }
 template <class O>
 __device__ __forceinline__ Weno5Inv<O> weno5_inv(
@@ -260,17 +266,26 @@ __device__ __forceinline__ Weno5Inv<O> weno5_inv(
   using S = typename O::S;
   using V = typename O::V;
   const V m2 = O::splat(S(-2)), k3 = O::splat(S(3)), m4 = O::splat(S(-4));
-  const V eps = O::splat(S(1e-6));
-  V b0 = weno5_beta<O>(O::add(O::fma(m2, vp1, v0), vp2),
-                       O::fma(m4, vp1, O::fma(k3, v0, vp2)));
-  V b1 = weno5_beta<O>(O::add(O::fma(m2, v0, vm1), vp1), O::sub(vm1, vp1));
-  V b2 = weno5_beta<O>(O::add(O::fma(m2, vm1, vm2), v0),
-                       O::fma(k3, v0, O::fma(m4, vm1, vm2)));
-  b0 = O::add(b0, eps);
-  b1 = O::add(b1, eps);
-  b2 = O::add(b2, eps);
+  const V b0 = weno5_b4<O>(O::add(O::fma(m2, vp1, v0), vp2),
+                           O::fma(m4, vp1, O::fma(k3, v0, vp2)));
+  const V b1 = weno5_b4<O>(O::add(O::fma(m2, v0, vm1), vp1), O::sub(vm1, vp1));
+  const V b2 = weno5_b4<O>(O::add(O::fma(m2, vm1, vm2), v0),
+                           O::fma(k3, v0, O::fma(m4, vm1, vm2)));
   return {O::rcp(O::mul(b0, b0)), O::rcp(O::mul(b1, b1)),
           O::rcp(O::mul(b2, b2))};
+}
+// sum i_r dq_r / sum d_r i_r for the weighted candidates dq_r = d_r q_r.
+template <class O>
+__device__ __forceinline__ typename O::V weno5_combine(
+    const Weno5Inv<O>& w, typename O::S d0, typename O::S d1,
+    typename O::S d2, typename O::V dq0, typename O::V dq1,
+    typename O::V dq2) {
+  const typename O::V num =
+      O::fma(w.i2, dq2, O::fma(w.i1, dq1, O::mul(w.i0, dq0)));
+  const typename O::V den =
+      O::fma(O::splat(d2), w.i2,
+             O::fma(O::splat(d1), w.i1, O::mul(O::splat(d0), w.i0)));
+  return O::mul(num, O::rcp(den));
 }
 template <class O>
 __device__ __forceinline__ typename O::V weno5_right_v(
@@ -278,20 +293,18 @@ __device__ __forceinline__ typename O::V weno5_right_v(
     typename O::V v0, typename O::V vp1, typename O::V vp2) {
   using S = typename O::S;
   using V = typename O::V;
-  const V a0 = O::mul(O::splat(S(0.3)), w.i0);
-  const V a1 = O::mul(O::splat(S(0.6)), w.i1);
-  const V a2 = O::mul(O::splat(S(0.1)), w.i2);
-  const V q0 = O::fma(O::splat(S(-1.0 / 6.0)), vp2,
-                      O::fma(O::splat(S(5.0 / 6.0)), vp1,
-                             O::mul(O::splat(S(1.0 / 3.0)), v0)));
-  const V q1 = O::fma(O::splat(S(1.0 / 3.0)), vp1,
-                      O::fma(O::splat(S(5.0 / 6.0)), v0,
-                             O::mul(O::splat(S(-1.0 / 6.0)), vm1)));
-  const V q2 = O::fma(O::splat(S(11.0 / 6.0)), v0,
-                      O::fma(O::splat(S(-7.0 / 6.0)), vm1,
-                             O::mul(O::splat(S(1.0 / 3.0)), vm2)));
-  const V num = O::fma(a2, q2, O::fma(a1, q1, O::mul(a0, q0)));
-  return O::mul(num, O::rcp(O::add(O::add(a0, a1), a2)));
+  // 0.3 q0, 0.6 q1, 0.1 q2 with q0 = (2 v0 + 5 vp1 - vp2) / 6,
+  // q1 = (-vm1 + 5 v0 + 2 vp1) / 6, q2 = (2 vm2 - 7 vm1 + 11 v0) / 6.
+  const V dq0 = O::fma(O::splat(S(-0.05)), vp2,
+                       O::fma(O::splat(S(0.25)), vp1,
+                              O::mul(O::splat(S(0.1)), v0)));
+  const V dq1 = O::fma(O::splat(S(0.2)), vp1,
+                       O::fma(O::splat(S(0.5)), v0,
+                              O::mul(O::splat(S(-0.1)), vm1)));
+  const V dq2 = O::fma(O::splat(S(11.0 / 60.0)), v0,
+                       O::fma(O::splat(S(-7.0 / 60.0)), vm1,
+                              O::mul(O::splat(S(1.0 / 30.0)), vm2)));
+  return weno5_combine<O>(w, S(0.3), S(0.6), S(0.1), dq0, dq1, dq2);
 }
 template <class O>
 __device__ __forceinline__ typename O::V weno5_left_v(
@@ -299,20 +312,18 @@ __device__ __forceinline__ typename O::V weno5_left_v(
     typename O::V v0, typename O::V vp1, typename O::V vp2) {
   using S = typename O::S;
   using V = typename O::V;
-  const V a0 = O::mul(O::splat(S(0.1)), w.i0);
-  const V a1 = O::mul(O::splat(S(0.6)), w.i1);
-  const V a2 = O::mul(O::splat(S(0.3)), w.i2);
-  const V q0 = O::fma(O::splat(S(1.0 / 3.0)), vp2,
-                      O::fma(O::splat(S(-7.0 / 6.0)), vp1,
-                             O::mul(O::splat(S(11.0 / 6.0)), v0)));
-  const V q1 = O::fma(O::splat(S(-1.0 / 6.0)), vp1,
-                      O::fma(O::splat(S(5.0 / 6.0)), v0,
-                             O::mul(O::splat(S(1.0 / 3.0)), vm1)));
-  const V q2 = O::fma(O::splat(S(1.0 / 3.0)), v0,
-                      O::fma(O::splat(S(5.0 / 6.0)), vm1,
-                             O::mul(O::splat(S(-1.0 / 6.0)), vm2)));
-  const V num = O::fma(a2, q2, O::fma(a1, q1, O::mul(a0, q0)));
-  return O::mul(num, O::rcp(O::add(O::add(a0, a1), a2)));
+  // 0.1 q0, 0.6 q1, 0.3 q2 with q0 = (11 v0 - 7 vp1 + 2 vp2) / 6,
+  // q1 = (2 vm1 + 5 v0 - vp1) / 6, q2 = (-vm2 + 5 vm1 + 2 v0) / 6.
+  const V dq0 = O::fma(O::splat(S(1.0 / 30.0)), vp2,
+                       O::fma(O::splat(S(-7.0 / 60.0)), vp1,
+                              O::mul(O::splat(S(11.0 / 60.0)), v0)));
+  const V dq1 = O::fma(O::splat(S(-0.1)), vp1,
+                       O::fma(O::splat(S(0.5)), v0,
+                              O::mul(O::splat(S(0.2)), vm1)));
+  const V dq2 = O::fma(O::splat(S(0.1)), v0,
+                       O::fma(O::splat(S(0.25)), vm1,
+                              O::mul(O::splat(S(-0.05)), vm2)));
+  return weno5_combine<O>(w, S(0.1), S(0.6), S(0.3), dq0, dq1, dq2);
 }
 
 // WENO3 (k = 2) on v[c-1..c+1]: reciprocals of (eps + beta_r)^2, then the
