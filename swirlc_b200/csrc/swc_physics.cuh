@@ -242,7 +242,8 @@ struct Two<double> {
 // beta_r = 13/12 a_r^2 + 1/4 b_r^2 and the candidate polynomials q_r of the
 // reference prototype's `weno5`; the value is sum alpha_r q_r / sum alpha_r.
 // Computed as: B_r = 4 (beta_r + eps) = 13/3 a_r^2 + (b_r^2 + 4 eps) (eps
-// folds into an FMA), i_r = 1/B_r^2 (shared by both faces of the cell), and
+// folds into an FMA; a_r, b_r from first differences, below),
+// i_r = 1/B_r^2 (shared by both faces of the cell), and
 // per face num = sum i_r (d_r q_r), den = sum d_r i_r with d_r folded into
 // the candidates' coefficients. The common factor 1/16 of i_r cancels in
 // num/den, so the weights are the prototype's in exact arithmetic.
@@ -251,26 +252,42 @@ template <class O>
 struct Weno5Inv {
   typename O::V i0, i1, i2;
 };
-// 4 (beta + eps) from the stencil differences a and b.
+// The indicators are built from the first differences e_k = v[k+1] - v[k]
+// of the stencil: a_r is the second difference of candidate r's three cells
+// (e_hi - e_lo), so two neighbouring cells' indicators share two of their
+// three (a_r, 13/3 a_r) pairs; b_r = e_hi - 3 e_lo (r = 0), e_lo + e_hi
+// (r = 1) and e_lo - 3 e_hi (r = 2) up to sign.
 template <class O>
-__device__ __forceinline__ typename O::V weno5_b4(typename O::V a,
+struct Weno5Tri {  // second difference a of three cells and 13/3 a
+  typename O::V a, ca;
+};
+template <class O>
+__device__ __forceinline__ Weno5Tri<O> weno5_tri(typename O::V e_lo,
+                                                 typename O::V e_hi) {
+  using S = typename O::S;
+  const typename O::V a = O::sub(e_hi, e_lo);
+  return {a, O::mul(O::splat(S(13.0 / 3.0)), a)};
+}
+// 4 (beta + eps) = 13/3 a^2 + (b^2 + 4 eps).
+template <class O>
+__device__ __forceinline__ typename O::V weno5_b4(const Weno5Tri<O>& t,
                                                   typename O::V b) {
   using S = typename O::S;
-  return O::fma(O::mul(O::splat(S(13.0 / 3.0)), a), a,
-                O::fma(b, b, O::splat(S(4e-6))));
+  return O::fma(t.ca, t.a, O::fma(b, b, O::splat(S(4e-6))));
 }
+// Cell with differences dm2 = v[c-1]-v[c-2], dm1 = v[c]-v[c-1],
+// d0 = v[c+1]-v[c], d1 = v[c+2]-v[c+1] and the second differences
+// t2 = (dm2, dm1), t1 = (dm1, d0), t0 = (d0, d1).
 template <class O>
 __device__ __forceinline__ Weno5Inv<O> weno5_inv(
-    typename O::V vm2, typename O::V vm1, typename O::V v0, typename O::V vp1,
-    typename O::V vp2) {
+    const Weno5Tri<O>& t2, const Weno5Tri<O>& t1, const Weno5Tri<O>& t0,
+    typename O::V dm2, typename O::V dm1, typename O::V d0,
+    typename O::V d1) {
   using S = typename O::S;
-  using V = typename O::V;
-  const V m2 = O::splat(S(-2)), k3 = O::splat(S(3)), m4 = O::splat(S(-4));
-  const V b0 = weno5_b4<O>(O::add(O::fma(m2, vp1, v0), vp2),
-                           O::fma(m4, vp1, O::fma(k3, v0, vp2)));
-  const V b1 = weno5_b4<O>(O::add(O::fma(m2, v0, vm1), vp1), O::sub(vm1, vp1));
-  const V b2 = weno5_b4<O>(O::add(O::fma(m2, vm1, vm2), v0),
-                           O::fma(k3, v0, O::fma(m4, vm1, vm2)));
+  const typename O::V m3 = O::splat(S(-3));
+  const typename O::V b0 = weno5_b4<O>(t0, O::fma(m3, d0, d1));
+  const typename O::V b1 = weno5_b4<O>(t1, O::add(d0, dm1));
+  const typename O::V b2 = weno5_b4<O>(t2, O::fma(m3, dm1, dm2));
   return {O::rcp(O::mul(b0, b0)), O::rcp(O::mul(b1, b1)),
           O::rcp(O::mul(b2, b2))};
 }
@@ -374,10 +391,20 @@ __device__ __forceinline__ void recon_face(const typename O::V* s, int limiter,
                                            typename O::V& pos) {
   using S = typename O::S;
   if constexpr (SCHEME == 0) {
-    neg = weno5_right_v<O>(weno5_inv<O>(s[0], s[1], s[2], s[3], s[4]), s[0],
-                           s[1], s[2], s[3], s[4]);
-    pos = weno5_left_v<O>(weno5_inv<O>(s[1], s[2], s[3], s[4], s[5]), s[1],
-                          s[2], s[3], s[4], s[5]);
+    // Cells i-1 (s[0..4]) and i (s[1..5]) share the differences e1..e3
+    // and the second differences f1, f2.
+    typename O::V e[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) e[k] = O::sub(s[k + 1], s[k]);
+    Weno5Tri<O> f[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) f[k] = weno5_tri<O>(e[k], e[k + 1]);
+    neg = weno5_right_v<O>(
+        weno5_inv<O>(f[0], f[1], f[2], e[0], e[1], e[2], e[3]), s[0], s[1],
+        s[2], s[3], s[4]);
+    pos = weno5_left_v<O>(
+        weno5_inv<O>(f[1], f[2], f[3], e[1], e[2], e[3], e[4]), s[1], s[2],
+        s[3], s[4], s[5]);
   } else if constexpr (SCHEME == 1) {
     typename O::V i0, i1;
     weno3_inv<O>(s[0], s[1], s[2], i0, i1);
@@ -402,7 +429,12 @@ __device__ __forceinline__ void recon_cell(const typename O::V* s, int limiter,
                                            typename O::V& right) {
   using S = typename O::S;
   if constexpr (SCHEME == 0) {
-    const Weno5Inv<O> w = weno5_inv<O>(s[0], s[1], s[2], s[3], s[4]);
+    typename O::V e[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) e[k] = O::sub(s[k + 1], s[k]);
+    const Weno5Inv<O> w = weno5_inv<O>(
+        weno5_tri<O>(e[0], e[1]), weno5_tri<O>(e[1], e[2]),
+        weno5_tri<O>(e[2], e[3]), e[0], e[1], e[2], e[3]);
     right = weno5_right_v<O>(w, s[0], s[1], s[2], s[3], s[4]);
     left = weno5_left_v<O>(w, s[0], s[1], s[2], s[3], s[4]);
   } else if constexpr (SCHEME == 1) {
