@@ -103,6 +103,17 @@ class ClockSampler:
           stdout=open(self.path, 'w'), stderr=subprocess.DEVNULL)
     except OSError:
       self.proc = None
+      return
+    # Start timing only once samples flow (nvidia-smi takes a moment to
+    # start), so that the timed region is covered; at most 5 s.
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+      try:
+        if os.path.getsize(self.path) > 0:
+          break
+      except OSError:
+        break
+      time.sleep(0.02)
 
   def stop(self):
     if self.proc is None:
@@ -863,7 +874,7 @@ def run_reference(args):
 def main():
   ap = argparse.ArgumentParser()
   ap.add_argument('--gpus', type=int, default=1)
-  ap.add_argument('--steps', type=int, default=20)
+  ap.add_argument('--steps', type=int, default=50)
   ap.add_argument('--warmup', type=int, default=3)
   ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
   ap.add_argument('--n', type=int, default=N_CELLS_EDGE)
