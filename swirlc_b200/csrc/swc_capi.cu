@@ -77,6 +77,57 @@ __global__ void halo_kernel(const HaloArgs a) {
     halo_elem<T>(a, t);
 }
 
+// Halo fill of fields that are periodic in all three dims, in one pass: each
+// halo cell copies the interior cell it wraps to. The x, y, z passes of
+// halo_kernel compose to exactly this copy when every dim is periodic and
+// no halo is wider than the interior (each pass copies interior layers,
+// and a corner's value reaches it through the other dims' copies). Thread
+// t < 2h planes of nxa*nya cells takes a whole z-halo plane cell; the rest
+// take the x/y frame (2h full rows, then 2h cells of each interior row) of
+// the interior planes. 32-bit indices (the caller checks the count).
+template <typename T>
+__global__ void halo_periodic_kernel(const HaloArgs a, int total) {
+  const int h = a.h, nx = a.nx, ny = a.ny, nz = a.nz;
+  const int nxa = nx + 2 * h, nya = ny + 2 * h;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  const int plane = nxa * nya;
+  const int frame = 2 * h * nya + nx * 2 * h;
+  int xa, ya, za;
+  if (t < 2 * h * plane) {
+    const int zi = t / plane, r = t - zi * plane;
+    za = zi < h ? zi : nz + zi;
+    xa = r / nya;
+    ya = r - xa * nya;
+  } else {
+    const int u = t - 2 * h * plane;
+    const int zi = u / frame;
+    int r = u - zi * frame;
+    za = h + zi;
+    if (r < 2 * h * nya) {
+      const int row = r / nya;
+      ya = r - row * nya;
+      xa = row < h ? row : nx + row;
+    } else {
+      r -= 2 * h * nya;
+      const int q = r / (2 * h), j = r - q * (2 * h);
+      xa = h + q;
+      ya = j < h ? j : ny + j;
+    }
+  }
+  auto wrap = [h](int c, int n) { return c < h ? c + n : (c >= n + h ? c - n : c); };
+  const long long o = za * a.sz + xa * a.sx + ya;
+  const long long os = wrap(za, nz) * a.sz + wrap(xa, nx) * a.sx + wrap(ya, ny);
+  // Every load before any store (the compiler cannot tell the fields apart).
+  T v[SWC_MAX_FIELDS];
+#pragma unroll
+  for (int f = 0; f < SWC_MAX_FIELDS; ++f)
+    if (f < a.nf) v[f] = static_cast<const T*>(a.fld[f].f)[os];
+#pragma unroll
+  for (int f = 0; f < SWC_MAX_FIELDS; ++f)
+    if (f < a.nf) static_cast<T*>(a.fld[f].f)[o] = v[f];
+}
+
 
 // ---------------------------------------------------------------------------
 // CFL reduction, device clock.
@@ -344,6 +395,34 @@ int swc_halo_fill(const SwcGrid* grid, int32_t dtype, int32_t nfields,
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int h = grid->halo;
   if (h == 0) return SWC_OK;
+  {
+    // Every field periodic in every dim, no primitive BCs, halos no wider
+    // than the interior: one pass instead of three.
+    bool all_periodic = !any_prim && h <= grid->nx && h <= grid->ny && h <= grid->nz;
+    for (int i = 0; i < nfields && all_periodic; ++i)
+      for (int d = 0; d < 3; ++d)
+        all_periodic = all_periodic && (bcs[i].side[d][0].kind == SWC_BC_PERIODIC ||
+                                        bcs[i].side[d][1].kind == SWC_BC_PERIODIC);
+    const long long nxa = grid->nx + 2LL * h, nya = grid->ny + 2LL * h;
+    const long long total = 2LL * h * nxa * nya +
+                            (long long)grid->nz * (2LL * h * nya + 2LL * h * grid->nx);
+    if (all_periodic && total < (1LL << 31)) {
+      HaloArgs a;
+      memset(&a, 0, sizeof(a));
+      a.nf = nfields;
+      for (int i = 0; i < nfields; ++i) a.fld[i].f = fields[i];
+      a.nx = grid->nx; a.ny = grid->ny; a.nz = grid->nz; a.h = h;
+      a.sx = grid->sx; a.sz = grid->sz;
+      const int threads = 256;
+      const unsigned blocks = (unsigned)((total + threads - 1) / threads);
+      if (dtype == SWC_F32)
+        halo_periodic_kernel<float><<<blocks, threads, 0, s>>>(a, (int)total);
+      else
+        halo_periodic_kernel<double><<<blocks, threads, 0, s>>>(a, (int)total);
+      note_launch();
+      return check_launch("halo_fill");
+    }
+  }
   // Phase 0: fields with direct BCs; phase 1: fields with primitive BCs,
   // after rho is complete in all three dims.
   for (int phase = 0; phase < (any_prim ? 2 : 1); ++phase) {
