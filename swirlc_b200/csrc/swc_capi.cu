@@ -77,16 +77,19 @@ __global__ void halo_kernel(const HaloArgs a) {
     halo_elem<T>(a, t);
 }
 
-// Halo fill of fields that are periodic in all three dims, in one pass: each
-// halo cell copies the interior cell it wraps to. The x, y, z passes of
-// halo_kernel compose to exactly this copy when every dim is periodic and
-// no halo is wider than the interior (each pass copies interior layers,
-// and a corner's value reaches it through the other dims' copies). Thread
+// Halo fill, in one pass, of fields whose every dim is periodic (clamp[d] =
+// 0) or zero-gradient (Neumann with value 0 on both sides, clamp[d] = 1):
+// each halo cell copies the interior cell it wraps to, or the edge cell it
+// clamps to. The x, y, z passes of halo_kernel compose to exactly this copy
+// when no halo is wider than the interior (each pass copies interior
+// layers, a Neumann layer with increment 0 is its edge value, and a
+// corner's value reaches it through the other dims' copies). Thread
 // t < 2h planes of nxa*nya cells takes a whole z-halo plane cell; the rest
 // take the x/y frame (2h full rows, then 2h cells of each interior row) of
 // the interior planes. 32-bit indices (the caller checks the count).
 template <typename T>
-__global__ void halo_periodic_kernel(const HaloArgs a, int total) {
+__global__ void halo_periodic_kernel(const HaloArgs a, int total,
+                                     int clamp_x, int clamp_y, int clamp_z) {
   const int h = a.h, nx = a.nx, ny = a.ny, nz = a.nz;
   const int nxa = nx + 2 * h, nya = ny + 2 * h;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -115,9 +118,13 @@ __global__ void halo_periodic_kernel(const HaloArgs a, int total) {
       ya = j < h ? j : ny + j;
     }
   }
-  auto wrap = [h](int c, int n) { return c < h ? c + n : (c >= n + h ? c - n : c); };
+  auto src = [h](int c, int n, int clamp) {
+    if (clamp) return c < h ? h : (c >= n + h ? n + h - 1 : c);
+    return c < h ? c + n : (c >= n + h ? c - n : c);
+  };
   const long long o = za * a.sz + xa * a.sx + ya;
-  const long long os = wrap(za, nz) * a.sz + wrap(xa, nx) * a.sx + wrap(ya, ny);
+  const long long os = src(za, nz, clamp_z) * a.sz +
+                       src(xa, nx, clamp_x) * a.sx + src(ya, ny, clamp_y);
   // Every load before any store (the compiler cannot tell the fields apart).
   T v[SWC_MAX_FIELDS];
 #pragma unroll
@@ -396,13 +403,26 @@ int swc_halo_fill(const SwcGrid* grid, int32_t dtype, int32_t nfields,
   const int h = grid->halo;
   if (h == 0) return SWC_OK;
   {
-    // Every field periodic in every dim, no primitive BCs, halos no wider
-    // than the interior: one pass instead of three.
+    // Every dim periodic for every field, or zero-gradient for every
+    // field, no primitive BCs, halos no wider than the interior: one pass
+    // instead of three.
     bool all_periodic = !any_prim && h <= grid->nx && h <= grid->ny && h <= grid->nz;
-    for (int i = 0; i < nfields && all_periodic; ++i)
-      for (int d = 0; d < 3; ++d)
-        all_periodic = all_periodic && (bcs[i].side[d][0].kind == SWC_BC_PERIODIC ||
-                                        bcs[i].side[d][1].kind == SWC_BC_PERIODIC);
+    int clamp[3] = {0, 0, 0};
+    for (int d = 0; d < 3 && all_periodic; ++d) {
+      int n_per = 0, n_zero = 0;
+      for (int i = 0; i < nfields; ++i) {
+        const SwcBC& lo = bcs[i].side[d][0];
+        const SwcBC& hi = bcs[i].side[d][1];
+        if (lo.kind == SWC_BC_PERIODIC || hi.kind == SWC_BC_PERIODIC) ++n_per;
+        else if (lo.kind == SWC_BC_NEUMANN && hi.kind == SWC_BC_NEUMANN &&
+                 lo.value == 0.0 && hi.value == 0.0 && !lo.per_layer &&
+                 !hi.per_layer)
+          ++n_zero;
+      }
+      if (n_per == nfields) clamp[d] = 0;
+      else if (n_zero == nfields) clamp[d] = 1;
+      else all_periodic = false;
+    }
     const long long nxa = grid->nx + 2LL * h, nya = grid->ny + 2LL * h;
     const long long total = 2LL * h * nxa * nya +
                             (long long)grid->nz * (2LL * h * nya + 2LL * h * grid->nx);
@@ -416,9 +436,11 @@ int swc_halo_fill(const SwcGrid* grid, int32_t dtype, int32_t nfields,
       const int threads = 256;
       const unsigned blocks = (unsigned)((total + threads - 1) / threads);
       if (dtype == SWC_F32)
-        halo_periodic_kernel<float><<<blocks, threads, 0, s>>>(a, (int)total);
+        halo_periodic_kernel<float><<<blocks, threads, 0, s>>>(
+            a, (int)total, clamp[0], clamp[1], clamp[2]);
       else
-        halo_periodic_kernel<double><<<blocks, threads, 0, s>>>(a, (int)total);
+        halo_periodic_kernel<double><<<blocks, threads, 0, s>>>(
+            a, (int)total, clamp[0], clamp[1], clamp[2]);
       note_launch();
       return check_launch("halo_fill");
     }
