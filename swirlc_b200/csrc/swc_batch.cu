@@ -24,6 +24,18 @@ struct HaloBatch {
   int bpre[SWC_BATCH_CHUNK + 1];
   HaloMember m[SWC_BATCH_CHUNK];
 };
+// One-pass halo fill (halo_shell_elem) of up to SWC_BATCH_CHUNK members:
+// block b serves member m with bpre[m] <= b < bpre[m+1].
+struct ShellMember {
+  HaloMember g;
+  int clamp[3];
+  int total;  // cells of the member's halo shell
+};
+struct ShellBatch {
+  int n;
+  int bpre[SWC_BATCH_CHUNK + 1];
+  ShellMember m[SWC_BATCH_CHUNK];
+};
 struct ClockBatch {
   int n;
   SwcClock* c[SWC_BATCH_CHUNK];
@@ -51,6 +63,22 @@ __global__ void halo_batch_kernel(const HaloBatch b) {
   for (long long i = (long long)(t - b.bpre[lo]) * blockDim.x + threadIdx.x;
        i < total; i += (long long)nb * blockDim.x)
     halo_elem<T>(a, i);
+}
+
+template <typename T>
+__global__ void shell_batch_kernel(const ShellBatch b) {
+  const int t = blockIdx.x;
+  int lo = 0, hi = b.n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (b.bpre[mid] <= t) lo = mid;
+    else hi = mid;
+  }
+  const ShellMember& m = b.m[lo];
+  const int nb = b.bpre[lo + 1] - b.bpre[lo];
+  for (int i = (t - b.bpre[lo]) * blockDim.x + threadIdx.x; i < m.total;
+       i += nb * blockDim.x)
+    halo_shell_elem<T>(m.g, i, m.clamp[0], m.clamp[1], m.clamp[2]);
 }
 
 __global__ void clock_batch_kernel(const ClockBatch b, int end) {
@@ -116,6 +144,45 @@ int check_member(const SwcBatchMember& m, int i, int need) {
 }
 
 template <typename T>
+int launch_shell(const ShellBatch& b, cudaStream_t s) {
+  if (b.n == 0) return SWC_OK;
+  shell_batch_kernel<T><<<b.bpre[b.n], kHaloThreads, 0, s>>>(b);
+  note_launch();
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess
+             ? SWC_OK
+             : record_error(SWC_ERR_LAUNCH, "batch halo: %s", cudaGetErrorString(e));
+}
+
+// Whether member m's halos can be filled in one pass (every dim periodic for
+// all 5 fields, or zero-gradient for all of them; no primitive BCs; halos no
+// wider than the interior), and with which clamp flags.
+bool shell_ok(const SwcBatchMember& m, int clamp[3]) {
+  const int h = m.grid.halo;
+  if (h <= 0 || h > m.grid.nx || h > m.grid.ny || h > m.grid.nz) return false;
+  if (halo_shell_count(m.grid.nx, m.grid.ny, m.grid.nz, h) >= (1LL << 31))
+    return false;
+  for (int v = 0; v < 5; ++v)
+    if (m.bcs[v].via_primitive) return false;
+  for (int d = 0; d < 3; ++d) {
+    int n_per = 0, n_zero = 0;
+    for (int v = 0; v < 5; ++v) {
+      const SwcBC& lo = m.bcs[v].side[d][0];
+      const SwcBC& hi = m.bcs[v].side[d][1];
+      if (lo.kind == SWC_BC_PERIODIC || hi.kind == SWC_BC_PERIODIC) ++n_per;
+      else if (lo.kind == SWC_BC_NEUMANN && hi.kind == SWC_BC_NEUMANN &&
+               lo.value == 0.0 && hi.value == 0.0 && !lo.per_layer &&
+               !hi.per_layer)
+        ++n_zero;
+    }
+    if (n_per == 5) clamp[d] = 0;
+    else if (n_zero == 5) clamp[d] = 1;
+    else return false;
+  }
+  return true;
+}
+
+template <typename T>
 int launch_halo(const HaloBatch& b, cudaStream_t s) {
   if (b.n == 0) return SWC_OK;
   halo_batch_kernel<T><<<b.bpre[b.n], kHaloThreads, 0, s>>>(b);
@@ -131,6 +198,40 @@ int launch_halo(const HaloBatch& b, cudaStream_t s) {
 // swc_halo_fill does for one grid with rho at index 0.
 int batch_halo(const std::vector<Plan>& plans, int set, int dtype,
                cudaStream_t s) {
+  // Members whose halos take one pass go through shell_batch_kernel; the
+  // others through the x, y, z passes below.
+  std::vector<char> shell(plans.size(), 0);
+  {
+    ShellBatch sb;
+    memset(&sb, 0, sizeof(sb));
+    for (size_t i = 0; i < plans.size(); ++i) {
+      const SwcBatchMember& m = *plans[i].m;
+      int clamp[3];
+      if (!shell_ok(m, clamp)) continue;
+      shell[i] = 1;
+      ShellMember& sm = sb.m[sb.n];
+      memset(&sm, 0, sizeof(sm));
+      sm.g.nf = 5;
+      for (int v = 0; v < 5; ++v) sm.g.fld[v].f = field_of(m, set, v);
+      sm.g.nx = m.grid.nx; sm.g.ny = m.grid.ny; sm.g.nz = m.grid.nz;
+      sm.g.h = m.grid.halo;
+      sm.g.sx = m.grid.sx; sm.g.sz = m.grid.sz;
+      for (int d = 0; d < 3; ++d) sm.clamp[d] = clamp[d];
+      sm.total = (int)halo_shell_count(m.grid.nx, m.grid.ny, m.grid.nz, m.grid.halo);
+      const int nb = (int)std::min<long long>(
+          kHaloMaxBlocksPerMember, (sm.total + kHaloThreads - 1) / kHaloThreads);
+      sb.bpre[sb.n + 1] = sb.bpre[sb.n] + nb;
+      if (++sb.n == SWC_BATCH_CHUNK) {
+        const int rc = dtype == SWC_F32 ? launch_shell<float>(sb, s)
+                                        : launch_shell<double>(sb, s);
+        if (rc) return rc;
+        memset(&sb, 0, sizeof(sb));
+      }
+    }
+    const int rc = dtype == SWC_F32 ? launch_shell<float>(sb, s)
+                                    : launch_shell<double>(sb, s);
+    if (rc) return rc;
+  }
   bool any_prim = false;
   for (const Plan& p : plans)
     for (int v = 0; v < 5; ++v) any_prim |= p.m->bcs[v].via_primitive != 0;
@@ -138,8 +239,9 @@ int batch_halo(const std::vector<Plan>& plans, int set, int dtype,
   for (int phase = 0; phase < (any_prim ? 2 : 1); ++phase) {
     for (int d = 0; d < 3; ++d) {
       memset(&b, 0, sizeof(b));
-      for (const Plan& p : plans) {
-        const SwcBatchMember& m = *p.m;
+      for (size_t pi = 0; pi < plans.size(); ++pi) {
+        if (shell[pi]) continue;
+        const SwcBatchMember& m = *plans[pi].m;
         if (m.grid.halo == 0) continue;
         HaloMember hm;
         memset(&hm, 0, sizeof(hm));

@@ -77,64 +77,13 @@ __global__ void halo_kernel(const HaloArgs a) {
     halo_elem<T>(a, t);
 }
 
-// Halo fill, in one pass, of fields whose every dim is periodic (clamp[d] =
-// 0) or zero-gradient (Neumann with value 0 on both sides, clamp[d] = 1):
-// each halo cell copies the interior cell it wraps to, or the edge cell it
-// clamps to. The x, y, z passes of halo_kernel compose to exactly this copy
-// when no halo is wider than the interior (each pass copies interior
-// layers, a Neumann layer with increment 0 is its edge value, and a
-// corner's value reaches it through the other dims' copies). Thread
-// t < 2h planes of nxa*nya cells takes a whole z-halo plane cell; the rest
-// take the x/y frame (2h full rows, then 2h cells of each interior row) of
-// the interior planes. 32-bit indices (the caller checks the count).
+// One-pass halo fill of one grid (halo_shell_elem, swc_halo.cuh).
 template <typename T>
 __global__ void halo_periodic_kernel(const HaloArgs a, int total,
                                      int clamp_x, int clamp_y, int clamp_z) {
-  const int h = a.h, nx = a.nx, ny = a.ny, nz = a.nz;
-  const int nxa = nx + 2 * h, nya = ny + 2 * h;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= total) return;
-  const int plane = nxa * nya;
-  const int frame = 2 * h * nya + nx * 2 * h;
-  int xa, ya, za;
-  if (t < 2 * h * plane) {
-    const int zi = t / plane, r = t - zi * plane;
-    za = zi < h ? zi : nz + zi;
-    xa = r / nya;
-    ya = r - xa * nya;
-  } else {
-    const int u = t - 2 * h * plane;
-    const int zi = u / frame;
-    int r = u - zi * frame;
-    za = h + zi;
-    if (r < 2 * h * nya) {
-      const int row = r / nya;
-      ya = r - row * nya;
-      xa = row < h ? row : nx + row;
-    } else {
-      r -= 2 * h * nya;
-      const int q = r / (2 * h), j = r - q * (2 * h);
-      xa = h + q;
-      ya = j < h ? j : ny + j;
-    }
-  }
-  auto src = [h](int c, int n, int clamp) {
-    if (clamp) return c < h ? h : (c >= n + h ? n + h - 1 : c);
-    return c < h ? c + n : (c >= n + h ? c - n : c);
-  };
-  const long long o = za * a.sz + xa * a.sx + ya;
-  const long long os = src(za, nz, clamp_z) * a.sz +
-                       src(xa, nx, clamp_x) * a.sx + src(ya, ny, clamp_y);
-  // Every load before any store (the compiler cannot tell the fields apart).
-  T v[SWC_MAX_FIELDS];
-#pragma unroll
-  for (int f = 0; f < SWC_MAX_FIELDS; ++f)
-    if (f < a.nf) v[f] = static_cast<const T*>(a.fld[f].f)[os];
-#pragma unroll
-  for (int f = 0; f < SWC_MAX_FIELDS; ++f)
-    if (f < a.nf) static_cast<T*>(a.fld[f].f)[o] = v[f];
+  if (t < total) halo_shell_elem<T>(a, t, clamp_x, clamp_y, clamp_z);
 }
-
 
 // ---------------------------------------------------------------------------
 // CFL reduction, device clock.

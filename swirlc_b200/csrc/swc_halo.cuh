@@ -170,4 +170,70 @@ __device__ __forceinline__ void halo_elem(const A& a, long long t) {
   }
 }
 
+// Halo fill, in one pass, of fields whose every dim is periodic (clamp[d] =
+// 0) or zero-gradient (Neumann with value 0 on both sides, clamp[d] = 1):
+// each halo cell copies the interior cell it wraps to, or the edge cell it
+// clamps to. The x, y, z passes of halo_kernel compose to exactly this copy
+// when no halo is wider than the interior (each pass copies interior
+// layers, a Neumann layer with increment 0 is its edge value, and a
+// corner's value reaches it through the other dims' copies). Thread
+// t < 2h planes of nxa*nya cells takes a whole z-halo plane cell; the rest
+// take the x/y frame (2h full rows, then 2h cells of each interior row) of
+// the interior planes. 32-bit indices (the caller checks the count).
+//
+// Element t of the halo shell (t < halo_shell_count) of the grid in `a`
+// (HaloArgs or HaloMember).
+template <typename T, typename A>
+__device__ __forceinline__ void halo_shell_elem(const A& a, int t, int clamp_x,
+                                                int clamp_y, int clamp_z) {
+  constexpr int NFMAX = sizeof(A::fld) / sizeof(A::fld[0]);
+  const int h = a.h, nx = a.nx, ny = a.ny, nz = a.nz;
+  const int nxa = nx + 2 * h, nya = ny + 2 * h;
+  const int plane = nxa * nya;
+  const int frame = 2 * h * nya + nx * 2 * h;
+  int xa, ya, za;
+  if (t < 2 * h * plane) {
+    const int zi = t / plane, r = t - zi * plane;
+    za = zi < h ? zi : nz + zi;
+    xa = r / nya;
+    ya = r - xa * nya;
+  } else {
+    const int u = t - 2 * h * plane;
+    const int zi = u / frame;
+    int r = u - zi * frame;
+    za = h + zi;
+    if (r < 2 * h * nya) {
+      const int row = r / nya;
+      ya = r - row * nya;
+      xa = row < h ? row : nx + row;
+    } else {
+      r -= 2 * h * nya;
+      const int q = r / (2 * h), j = r - q * (2 * h);
+      xa = h + q;
+      ya = j < h ? j : ny + j;
+    }
+  }
+  auto src = [h](int c, int n, int clamp) {
+    if (clamp) return c < h ? h : (c >= n + h ? n + h - 1 : c);
+    return c < h ? c + n : (c >= n + h ? c - n : c);
+  };
+  const long long o = za * a.sz + xa * a.sx + ya;
+  const long long os = src(za, nz, clamp_z) * a.sz +
+                       src(xa, nx, clamp_x) * a.sx + src(ya, ny, clamp_y);
+  // Every load before any store (the compiler cannot tell the fields apart).
+  T v[NFMAX];
+#pragma unroll
+  for (int f = 0; f < NFMAX; ++f)
+    if (f < a.nf) v[f] = static_cast<const T*>(a.fld[f].f)[os];
+#pragma unroll
+  for (int f = 0; f < NFMAX; ++f)
+    if (f < a.nf) static_cast<T*>(a.fld[f].f)[o] = v[f];
+}
+
+// Cells of the halo shell of an (nx, ny, nz) grid with halo h.
+inline long long halo_shell_count(int nx, int ny, int nz, int h) {
+  const long long nxa = nx + 2LL * h, nya = ny + 2LL * h;
+  return 2LL * h * nxa * nya + (long long)nz * (2LL * h * nya + 2LL * h * nx);
+}
+
 }  // namespace swc
