@@ -242,9 +242,10 @@ typedef struct SwcBatchMember {
 /* One time step of every member (order 3: SSP-RK3, order 2: RK2), each with
  * the dt of its own clock, as swc_rk_step does for one grid. All members
  * share `scheme` (its pe_axis, tile and zseg are replaced by the members').
- * Each RK stage is one batched halo pass per dim and one batched stage
- * launch per tile shape over all members, instead of a launch sequence per
- * member. With 16x16 tiles each member's result equals swc_rk_step's bit for
+ * Each RK stage is one batched halo fill (one pass for members whose dims
+ * are all periodic or zero-gradient, else one pass per dim) and one batched
+ * stage launch per tile shape over all members, instead of a launch
+ * sequence per member. With 16x16 tiles each member's result equals swc_rk_step's bit for
  * bit; 8x32 tiles (for members at most 8 cells wide in y; not available for
  * f64 WENO5) can differ from it in the last bit. Members must not share
  * buffers. No counterpart in the reference, which advances
