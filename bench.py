@@ -145,6 +145,17 @@ class ClockSampler:
             'reasons': sorted(reasons), 'samples': len(sm)}
 
 
+def _kh_config(n, world):
+  """The `config` of the headline workload, shared by both arms."""
+  return {'workload': f'kelvin_helmholtz {n}^3 fp32 WENO5+HLLC+viscous, '
+                      'SSP-RK3, CFL 0.5, device dt',
+          'cells_per_gpu': n ** 3, 'halo_width': 3,
+          'parallelism': f'replicas x{world}',
+          'l2_flush': f'inputs larger than L2 (5 fields x {n + 6}^3 x 4 B '
+                      f'= {5 * (n + 6) ** 3 * 4 / 1e6:.0f} MB per state)',
+          'graph': 'one RK3 step captured in a CUDA graph'}
+
+
 def run_ours(args):
   import torch
   import torch.distributed as dist
@@ -272,7 +283,7 @@ def run_ours(args):
 
   cpu = None
   if rank == 0 and world == 1 and not args.no_cpu_baseline:
-    cpu = cpu_baseline_sample(args.cpu_sample)
+    cpu = cpu_baseline_slabs(n, procs=1, samples=2)
 
   if rank == 0:
     line = {
@@ -281,13 +292,7 @@ def run_ours(args):
         'ms_per_step': ms / args.steps, 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
         'data': 'synthetic (seeded KH initial condition, configs.kelvin_helmholtz)',
-        'config': {'workload': f'kelvin_helmholtz {n}^3 fp32 WENO5+HLLC+viscous, '
-                               'SSP-RK3, CFL 0.5, device dt',
-                   'cells_per_gpu': cells, 'halo_width': 3,
-                   'parallelism': f'replicas x{world}',
-                   'l2_flush': 'inputs larger than L2 (5 fields x 262^3 x 4 B '
-                               '= 360 MB per state)',
-                   'graph': 'one RK3 step captured in a CUDA graph'},
+        'config': _kh_config(n, world),
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak,
                      'unit': 'GB/s', 'frac': achieved / peak,
                      'peak_source': peak_kind,
@@ -758,12 +763,18 @@ def run_config_case(args):
 
 
 def run_profile(args):
-  """Eager RK3 steps of the workload, no timing: the command ncu captures."""
+  """Eager RK3 steps of the workload, no timing: the command ncu captures.
+  kh256: Kelvin-Helmholtz at --n^3; bubble: the buoyant bubble at
+  --n x --n x --n/2 (its 2:2:1 shape)."""
   import torch
   from swirlc_b200 import configs, engine
   from swirlc_b200.core import parameter
   from swirlc_b200.physics import physics_models
-  user_cfg, state = configs.kelvin_helmholtz(n=args.n)
+  if args.workload == 'bubble':
+    user_cfg, state = configs.buoyant_bubble(nx=args.n, ny=args.n,
+                                             nz=args.n // 2)
+  else:
+    user_cfg, state = configs.kelvin_helmholtz(n=args.n)
   cfg = parameter.SwirlCParameters(user_cfg)
   pm = physics_models.PhysicsModels(cfg)
   fields = [torch.tensor(state[k], device='cuda') for k in
@@ -775,7 +786,6 @@ def run_profile(args):
 
 
 def _oracle_rk3_worker(payload):
-  import numpy as _np
   from oracle import swirlc_oracle as orc
   cfg, state = payload
   t0 = time.perf_counter()
@@ -783,32 +793,76 @@ def _oracle_rk3_worker(payload):
   return time.perf_counter() - t0
 
 
-def cpu_baseline_sample(n_sample: int, procs: int = 1):
-  """Times the CPU oracle (NumPy float32) on one RK3 step of the KH set-up
-  at n_sample^3, `procs` independent samples in parallel processes."""
-  import multiprocessing as mp
-  from swirlc_b200 import configs
-  from oracle import swirlc_oracle as orc
-  user_cfg, state = configs.kelvin_helmholtz(n=n_sample)
-  keys = ('halo_width', 'dx', 'dy', 'dz', 'interpolation_scheme',
-          'numeric_flux_scheme', 'include_diffusion', 'transport_parameters',
-          'x', 'y', 'z', 'bc', 'dt')
-  ocfg = orc.make_cfg(**{k: user_cfg[k] for k in keys if k in user_cfg})
-  ocfg.bc = orc.periodic_bc()
-  if procs <= 1:
-    secs = _oracle_rk3_worker((ocfg, state))
-    total = n_sample ** 3 / secs
-  else:
-    ctx = mp.get_context('spawn')
-    with ctx.Pool(procs) as pool:
-      t0 = time.perf_counter()
-      pool.map(_oracle_rk3_worker, [(ocfg, state)] * procs)
-      secs = time.perf_counter() - t0
-    total = procs * n_sample ** 3 / secs
-  return {'value': total, 'unit': UNIT, 'cores': procs, 'kind': 'port',
-          'sample': f'one SSP-RK3 step of KH at {n_sample}^3 (WENO5+HLLC+'
-                    f'viscous) per process, NumPy float32 oracle, '
-                    f'{secs:.1f} s wall'}
+# z planes of the 256^3 grid one host process steps per sample.
+SLAB_PLANES = 8
+
+
+class KHSlabSampler:
+  """Times the CPU oracle (the NumPy float32 restatement of the reference
+  path) on z-slabs of the n^3 Kelvin-Helmholtz state.
+
+  One sample step: `procs` host processes each take one SSP-RK3 step of a
+  slab of SLAB_PLANES interior z planes of the full n x n cross-section
+  plus 3 halo planes on each side (the oracle evaluates its halo planes
+  too, so the rate counts interior cell-updates only and is conservative);
+  successive samples move through the domain. The pool is started with
+  `spawn` before any work.
+  """
+
+  def __init__(self, n: int, procs: int):
+    import multiprocessing as mp
+    from swirlc_b200 import configs
+    from oracle import swirlc_oracle as orc
+    self.n = n
+    self.procs = max(1, min(procs, n // SLAB_PLANES))
+    user_cfg, self.state = configs.kelvin_helmholtz(n=n)
+    keys = ('halo_width', 'dx', 'dy', 'dz', 'interpolation_scheme',
+            'numeric_flux_scheme', 'include_diffusion',
+            'transport_parameters', 'x', 'y', 'dt')
+    self.cfg = orc.make_cfg(**{k: user_cfg[k] for k in keys})
+    self.cfg.bc = orc.periodic_bc()
+    self.hw = user_cfg['halo_width']
+    self.pool = (mp.get_context('spawn').Pool(self.procs)
+                 if self.procs > 1 else None)
+    self.cells = self.procs * SLAB_PLANES * n * n
+
+  def _slab(self, z0: int):
+    idx = np.arange(z0, z0 + SLAB_PLANES + 2 * self.hw) % self.n + self.hw
+    return {k: np.ascontiguousarray(v[idx]) for k, v in self.state.items()}
+
+  def step(self, j: int) -> float:
+    """Wall seconds of sample step j."""
+    tasks = [(self.cfg, self._slab(((j * self.procs + p) * SLAB_PLANES) %
+                                   self.n)) for p in range(self.procs)]
+    t0 = time.perf_counter()
+    if self.pool is None:
+      _oracle_rk3_worker(tasks[0])
+    else:
+      self.pool.map(_oracle_rk3_worker, tasks)
+    return time.perf_counter() - t0
+
+  def describe(self) -> str:
+    return (f'one SSP-RK3 step of {self.procs} z-slab(s) of {SLAB_PLANES} '
+            f'planes x {self.n}^2 (+3 halo planes a side) of the KH '
+            f'{self.n}^3 state per sample, NumPy float32 oracle, '
+            f'{self.procs} process(es)')
+
+  def close(self):
+    if self.pool is not None:
+      self.pool.close()
+      self.pool.join()
+
+
+def cpu_baseline_slabs(n: int, procs: int = 1, samples: int = 2):
+  """The cpu_baseline object: the oracle on `samples` slab steps."""
+  sampler = KHSlabSampler(n, procs)
+  try:
+    secs = [sampler.step(j) for j in range(samples)]
+  finally:
+    sampler.close()
+  v = sampler.cells * len(secs) / sum(secs)
+  return {'value': v, 'unit': UNIT, 'cores': sampler.procs, 'kind': 'port',
+          'sample': sampler.describe() + f', {sum(secs):.1f} s wall'}
 
 
 def run_reference_batch(args):
@@ -839,30 +893,41 @@ def run_reference_batch(args):
 
 
 def run_reference(args):
+  """The reference arm: the CPU oracle on this host's cores, W warm-up and
+  K timed sample steps (KHSlabSampler), on the headline workload's config.
+  The reference's own TensorFlow path needs TensorFlow and swirl_lm, which
+  are not installed (no network); the oracle restates it."""
   rank, world, _ = _env_rank()
   if rank != 0:
     return
   if args.workload == 'riemann_batch':
     run_reference_batch(args)
     return
-  procs = os.cpu_count() or 1
-  vals = []
-  for _ in range(max(1, min(args.steps, 5))):
-    vals.append(cpu_baseline_sample(args.cpu_sample, procs))
-  v = statistics.median(x['value'] for x in vals)
-  base = vals[0]
+  try:
+    procs = len(os.sched_getaffinity(0))
+  except AttributeError:
+    procs = os.cpu_count() or 1
+  sampler = KHSlabSampler(args.n, procs)
+  try:
+    for j in range(args.warmup):
+      sampler.step(j)
+    secs = [sampler.step(args.warmup + j) for j in range(args.steps)]
+  finally:
+    sampler.close()
+  t = sum(secs)
+  v = sampler.cells * args.steps / t
   line = {
       'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': UNIT,
       'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
-      'ms_per_step': args.n ** 3 / v * 1e3, 'higher_is_better': True,
+      'ms_per_step': t / args.steps * 1e3, 'higher_is_better': True,
       'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
-      'data': 'synthetic (seeded KH initial condition)',
-      'config': {'workload': f'kelvin_helmholtz {args.n}^3 fp32 WENO5+HLLC+'
-                             'viscous, SSP-RK3 (CPU sample '
-                             f'{args.cpu_sample}^3 per process)',
-                 'parallelism': f'{procs} host processes'},
-      'cpu_baseline': {'value': v, 'unit': UNIT, 'cores': procs,
-                       'kind': 'port', 'sample': base['sample']},
+      'data': 'synthetic (seeded KH initial condition, configs.kelvin_helmholtz)',
+      'config': _kh_config(args.n, world),
+      'cpu_baseline': {'value': v, 'unit': UNIT, 'cores': sampler.procs,
+                       'kind': 'port',
+                       'sample': sampler.describe() + '; a step of this '
+                                 f'line is one sample ({sampler.cells} '
+                                 'interior cell-updates)'},
       'e2e': {'value': v, 'unit': UNIT, 'h2d_bytes_per_step': 0,
               'd2h_bytes_per_step': 0},
       'note': 'the reference TensorFlow path needs TensorFlow and swirl_lm, '
@@ -878,7 +943,6 @@ def main():
   ap.add_argument('--warmup', type=int, default=3)
   ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
   ap.add_argument('--n', type=int, default=N_CELLS_EDGE)
-  ap.add_argument('--cpu-sample', type=int, default=96)
   ap.add_argument('--no-cpu-baseline', action='store_true')
   ap.add_argument('--adj-n', type=int, default=128)
   ap.add_argument('--adj-steps', type=int, default=200)

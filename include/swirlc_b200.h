@@ -44,7 +44,8 @@ enum { SWC_F32 = 0, SWC_F64 = 1 };
 /* interpolation_scheme (compressible_navier_stokes.py:39-43); SWC_NODE is
  * the identity face value used by the reference tests' WENO mock. */
 enum { SWC_WENO5 = 0, SWC_WENO3 = 1, SWC_MUSCL = 2, SWC_NODE = 3 };
-enum { SWC_LIM_VAN_LEER = 0, SWC_LIM_MC = 1, SWC_LIM_MINMOD = 2 };
+enum { SWC_LIM_VAN_LEER = 0, SWC_LIM_MC = 1, SWC_LIM_MINMOD = 2,
+       SWC_LIM_MINMOD3 = 3 /* the prototype's three-slope minmod */ };
 /* numeric_flux_scheme (riemann_solver.py:24-27). */
 enum { SWC_HLL = 0, SWC_HLLC = 1 };
 /* BoundaryCondition (bc_types.py:22-27) plus NONE = leave the halo as is. */
@@ -217,7 +218,9 @@ int swc_rk_step(const SwcGrid* grid, const SwcScheme* scheme,
  * SWC_ERR_ARG before anything is launched (e.g. 96^3 f32 with halo 3 fits,
  * 128^3 does not). The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress with that device current); make that call
- * before any stream capture. All calls share the array, which keeps the last
+ * before any stream capture. The address is cached for the process: after a
+ * cudaDeviceReset it is stale and the entry point must not be called again
+ * in that process. All calls share the array, which keeps the last
  * call's contents, so calls that overlap on the GPU race: serialise them
  * (one stream, or events between streams and threads). Nothing in the array
  * needs to be zero; halo sides set to SWC_BC_NONE keep whatever the array
@@ -290,6 +293,17 @@ int swc_cfl_reduce(const SwcGrid* grid, const SwcScheme* scheme,
 int swc_clock_begin_step(SwcClock* clock_dev, void* stream);
 /* End of a step: t += dt, step += 1. */
 int swc_clock_end_step(SwcClock* clock_dev, void* stream);
+
+/* Non-finite detector (no reference counterpart: the reference's TF graph
+ * propagates NaN silently). The CFL reductions (swc_cfl_reduce and the one
+ * fused into the last stage of swc_rk_step / swc_batch_step) visit every
+ * new cell; a cell whose rho, p or rho_e is not finite, or whose CFL limit
+ * is NaN (p/rho < 0), contributes a limit of 0, which no finite state has.
+ * This call waits for `stream`, reads the clock and returns
+ * SWC_ERR_NONFINITE when clock->dtmin is 0 (the state after the last
+ * completed step is bad), else SWC_OK. It synchronises, so it is not for
+ * use inside stream capture; the step calls themselves stay asynchronous. */
+int swc_clock_status(const SwcClock* clock_dev, void* stream);
 
 /* Component kernels behind the reference's unit-level API. */
 

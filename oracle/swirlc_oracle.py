@@ -325,7 +325,7 @@ def weno(v, dim, k=3):
   return sh(right_face, dim, -1), left_face
 
 
-MUSCL_LIMITERS = ('van_leer', 'mc', 'minmod')
+MUSCL_LIMITERS = ('van_leer', 'mc', 'minmod', 'minmod3')
 
 
 def _limiter(r, kind):
@@ -349,17 +349,37 @@ def _limiter(r, kind):
   raise ValueError(f'Unknown limiter {kind}.')
 
 
+def _minmod3_slope(v, dim):
+  """The prototype's MUSCL slope (swirl_c_prototype.ipynb `muscl`, cell 4).
+
+  minmod of the central difference (v[c+1]-v[c-1])/(2*2) (its `central2`
+  with h = 2), the forward difference and the backward difference (h = 1):
+  s = mean of the three signs, the slope is s * min |.| where |s| == 1, else 0.
+  """
+  grads = ((sh(v, dim, 1) - sh(v, dim, -1)) / (2.0 * 2.0),
+           (sh(v, dim, 1) - v) / 1.0,
+           (v - sh(v, dim, -1)) / 1.0)
+  s = (np.sign(grads[0]) + np.sign(grads[1]) + np.sign(grads[2])) / 3
+  a_min = np.minimum(np.minimum(np.abs(grads[0]), np.abs(grads[1])),
+                     np.abs(grads[2]))
+  return np.where(np.abs(s) == 1, s * a_min, np.zeros_like(a_min)).astype(
+      v.dtype, copy=False)
+
+
 def muscl(v, dim, limiter='mc'):
   """Slope-limited MUSCL reconstruction at face i-1/2.
 
   For cell c: dp = v[c+1]-v[c], dm = v[c]-v[c-1], r = divide_no_nan(dm, dp),
-  slope = phi(r) * dp. neg[i] = v[i-1] + 0.5 slope[i-1];
-  pos[i] = v[i] - 0.5 slope[i].
+  slope = phi(r) * dp ('minmod3': the prototype's three-slope minmod).
+  neg[i] = v[i-1] + 0.5 slope[i-1]; pos[i] = v[i] - 0.5 slope[i].
   """
-  dp = sh(v, dim, 1) - v
-  dm = v - sh(v, dim, -1)
-  r = divide_no_nan(dm, dp)
-  slope = _limiter(r, limiter) * dp
+  if limiter == 'minmod3':
+    slope = _minmod3_slope(v, dim)
+  else:
+    dp = sh(v, dim, 1) - v
+    dm = v - sh(v, dim, -1)
+    r = divide_no_nan(dm, dp)
+    slope = _limiter(r, limiter) * dp
   right_face = v + 0.5 * slope
   left_face = v - 0.5 * slope
   return sh(right_face, dim, -1), left_face

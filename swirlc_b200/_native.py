@@ -28,7 +28,7 @@ SWC_ERR_NONFINITE = -5
 
 SWC_F32, SWC_F64 = 0, 1
 SWC_WENO5, SWC_WENO3, SWC_MUSCL, SWC_NODE = 0, 1, 2, 3
-SWC_LIM_VAN_LEER, SWC_LIM_MC, SWC_LIM_MINMOD = 0, 1, 2
+SWC_LIM_VAN_LEER, SWC_LIM_MC, SWC_LIM_MINMOD, SWC_LIM_MINMOD3 = 0, 1, 2, 3
 SWC_HLL, SWC_HLLC = 0, 1
 SWC_BC_PERIODIC, SWC_BC_DIRICHLET, SWC_BC_NEUMANN, SWC_BC_NONE = 0, 1, 2, 4
 SWC_OUT_RHS, SWC_OUT_EULER, SWC_OUT_CONVEX, SWC_OUT_AVERAGE = 0, 1, 2, 3
@@ -38,7 +38,7 @@ SWC_MAX_FIELDS = 8
 EXPORTED = (
     'swc_abi_version', 'swc_last_error', 'swc_launch_count', 'swc_halo_fill',
     'swc_rk_stage', 'swc_cfl_reduce', 'swc_clock_begin_step',
-    'swc_clock_end_step', 'swc_reconstruct', 'swc_riemann_flux',
+    'swc_clock_end_step', 'swc_clock_status', 'swc_reconstruct', 'swc_riemann_flux',
     'swc_wave_speeds', 'swc_stencil', 'swc_rk_combine', 'swc_rk_step',
     'swc_rk_step_noalloc', 'swc_batch_step', 'swc_rk_stage_ext',
     'swc_rk_stage_vjp',
@@ -146,6 +146,7 @@ def load(require_cuda: bool = True) -> ctypes.CDLL:
                                      ctypes.POINTER(SwcScheme), pp, vp, vp]
       lib.swc_clock_begin_step.argtypes = [vp, vp]
       lib.swc_clock_end_step.argtypes = [vp, vp]
+      lib.swc_clock_status.argtypes = [vp, vp]
       lib.swc_reconstruct.argtypes = [ctypes.POINTER(SwcGrid), i32, i32, i32,
                                       i32, vp, vp, vp, vp]
       lib.swc_riemann_flux.argtypes = [i64, i32, i32, i32, i32, pp, pp, vp, vp,
@@ -200,6 +201,8 @@ def check(rc: int, what: str = '') -> None:
     raise ValueError(msg)
   if rc == SWC_ERR_UNSUPPORTED:
     raise NotImplementedError(msg)
+  if rc == SWC_ERR_NONFINITE:
+    raise FloatingPointError(msg)
   raise RuntimeError(msg)
 
 

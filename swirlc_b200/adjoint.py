@@ -54,6 +54,9 @@ class RunAdjoint:
     self.order = 3 if scheme == 'rk3' else 2
     self.checkpoints: List[List[torch.Tensor]] = []
     self.dts: List[float] = []
+    # Incremented by every run(): the checkpoints, dts and stage buffers of
+    # a runner belong to its latest run only.
+    self.generation = 0
     self._scratch = [torch.empty(solver.shape, dtype=solver.dtype,
                                  device=solver.device)
                      for _ in range(nat.SWC_VJP_SCRATCH)]
@@ -117,6 +120,7 @@ class RunAdjoint:
           dts: Sequence[float]) -> List[torch.Tensor]:
     """Advances a copy of `fields` by len(dts) steps, keeping checkpoints."""
     self.s.check_fields(fields)
+    self.generation += 1
     self.dts = [float(d) for d in dts]
     u = [f.detach().clone() for f in fields]
     self.checkpoints = []
@@ -215,21 +219,35 @@ class RunAdjoint:
 
 
 class _Run(torch.autograd.Function):
-  """Forward run / reverse sweep as one autograd node."""
+  """Forward run / reverse sweep as one autograd node.
+
+  A runner holds the checkpoints of its latest run only, so it serves one
+  outstanding simulate() at a time: backward raises if the runner has run
+  again since this node's forward (use one RunAdjoint per live graph).
+  """
 
   @staticmethod
   def forward(ctx, runner, dts, nu, *fields):
     runner.s.scheme.nu = float(nu)
     out = runner.run(fields, dts)
     ctx.runner = runner
+    ctx.generation = runner.generation
+    ctx.nu_value = float(nu)
     ctx.nu_meta = (nu.dtype, nu.device)
     return tuple(out)
 
   @staticmethod
   def backward(ctx, *grads):
-    grads = [torch.zeros_like(ctx.runner._g[0][0]) if g is None else g
+    runner = ctx.runner
+    if runner.generation != ctx.generation:
+      raise RuntimeError(
+          'RunAdjoint has run again since this simulate() call; its '
+          'checkpoints now belong to the later run. Use one RunAdjoint per '
+          'simulate() whose backward is still pending.')
+    runner.s.scheme.nu = ctx.nu_value
+    grads = [torch.zeros_like(runner._g[0][0]) if g is None else g
              for g in grads]
-    gin, nub = ctx.runner.backward(grads)
+    gin, nub = runner.backward(grads)
     dtype, device = ctx.nu_meta
     return (None, None, torch.tensor(nub, dtype=dtype, device=device),
             *gin)

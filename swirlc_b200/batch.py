@@ -154,18 +154,25 @@ class BatchStepper:
     torch.cuda.current_stream().wait_stream(side)
     self.graph_steps = steps
 
-  def step(self, n: int = 1) -> None:
+  def step(self, n: int = 1, check: bool = False) -> None:
     """Advances every member by n steps (graph replays when captured; n must
-    then be a multiple of the captured step count)."""
+    then be a multiple of the captured step count). With `check`, waits and
+    raises FloatingPointError naming the first member whose new state holds
+    a non-finite rho, p or rho_e (swc_clock_status on its clock)."""
     if self.graph is None:
       for _ in range(n):
         self._launch_step()
-      return
-    if n % self.graph_steps:
-      raise ValueError(f'{n} steps is not a multiple of the captured '
-                       f'{self.graph_steps}.')
-    for _ in range(n // self.graph_steps):
-      self.graph.replay()
+    else:
+      if n % self.graph_steps:
+        raise ValueError(f'{n} steps is not a multiple of the captured '
+                         f'{self.graph_steps}.')
+      for _ in range(n // self.graph_steps):
+        self.graph.replay()
+    if check:
+      lib = nat.load()
+      for i, c in enumerate(self.clocks):
+        nat.check(lib.swc_clock_status(c.data_ptr(), nat.stream_ptr()),
+                  f'batch member {i}')
 
   # ------------------------------------------------------------ autotuner
   def _snapshot(self):

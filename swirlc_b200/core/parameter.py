@@ -5,7 +5,8 @@ reference and sets every key as an attribute, so a user cfg dict written for
 the reference builds the same object. Keys this implementation adds are
 optional and default to the reference's behaviour:
 
-  muscl_limiter  'van_leer' | 'mc' | 'minmod' (limiter of the MUSCL scheme)
+  muscl_limiter  'van_leer' | 'mc' | 'minmod' | 'minmod3' (limiter of the
+                 MUSCL scheme; 'minmod3' is the reference prototype's slope)
   cfl            > 0 turns on the device CFL time step (else cfg.dt is used)
   t_end          > 0 clamps the last CFL step to end at t_end
 """

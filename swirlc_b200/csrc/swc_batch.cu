@@ -42,6 +42,8 @@ struct ClockBatch {
 };
 static_assert(sizeof(HaloBatch) <= 32764, "halo member table too large");
 static_assert(sizeof(StageBatch) <= 32764, "stage member table too large");
+static_assert(sizeof(ShellBatch) <= 32764, "shell member table too large");
+static_assert(sizeof(ClockBatch) <= 32764, "clock table too large");
 
 // Block b serves the member m with bpre[m] <= b < bpre[m+1]; that member's
 // blocks stride over its halo elements.

@@ -127,7 +127,7 @@ __global__ void cfl_kernel(const CflArgs a) {
     T c = sqrt_(K<T>::gamma() * p / r);
     T l = min_(min_(T(a.dx) / (abs_(uu) + c), T(a.dy) / (abs_(vv) + c)),
                T(a.dz) / (abs_(ww) + c));
-    m = fmin(m, double(l));
+    m = fmin(m, cfl_limit_or_flag(r, p, u4[o], l));
   }
   __shared__ double red[32];
 #pragma unroll
@@ -685,6 +685,22 @@ int swc_clock_end_step(SwcClock* clock_dev, void* stream) {
   clock_end_kernel<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(clock_dev);
   note_launch();
   return check_launch("clock_end_step");
+}
+
+int swc_clock_status(const SwcClock* clock_dev, void* stream) {
+  if (!clock_dev) return fail(SWC_ERR_ARG, "clock is NULL");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  SwcClock c;
+  cudaError_t e = cudaMemcpyAsync(&c, clock_dev, sizeof(c), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess)
+    return fail(SWC_ERR_LAUNCH, "clock_status: %s", cudaGetErrorString(e));
+  if (c.dtmin == 0.0)
+    return fail(SWC_ERR_NONFINITE,
+                "non-finite or unphysical state (rho, p or rho_e not finite, "
+                "or p/rho < 0) after step %lld, t = %.9g",
+                (long long)c.step, c.t);
+  return SWC_OK;
 }
 
 int swc_reconstruct(const SwcGrid* grid, int32_t dtype, int32_t interp,

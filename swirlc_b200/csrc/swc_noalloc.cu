@@ -10,7 +10,10 @@
 // until the process exits. Its host-side name is not a device address, so the
 // first call on each device looks the address up with cudaGetSymbolAddress
 // while that device is current and caches it; that first call should come
-// before any stream capture. The array keeps whatever the last call left in
+// before any stream capture. The cached address belongs to the device's
+// primary context of that moment: after cudaDeviceReset (or any other
+// teardown of the primary context) it is stale, so this entry point must not
+// be called again in that process. The array keeps whatever the last call left in
 // it and is shared by all calls, so calls that overlap on the GPU (other
 // streams, other host threads on the same device) race on it. Nothing in it
 // has to start at zero: the step writes each work state's interior before

@@ -52,6 +52,24 @@ __device__ __forceinline__ float abs_(float a) { return fabsf(a); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double abs_(double a) { return fabs(a); }
+// Finite test on the exponent bits (unaffected by fast-math flags).
+__device__ __forceinline__ bool finite_(float a) {
+  return (__float_as_uint(a) & 0x7f800000u) != 0x7f800000u;
+}
+__device__ __forceinline__ bool finite_(double a) {
+  return (static_cast<unsigned long long>(__double_as_longlong(a)) &
+          0x7ff0000000000000ull) != 0x7ff0000000000000ull;
+}
+// CFL limit of one cell as it enters the min-reduction: delta_d/(|u_d|+c),
+// or 0 when rho, p or rho_e is not finite or the limit itself is NaN
+// (p/rho < 0). 0 is never a limit of a finite state, so a reduced minimum of
+// 0 reports a non-finite or unphysical state to the host
+// (swc_clock_status).
+template <typename T>
+__device__ __forceinline__ double cfl_limit_or_flag(T rho, T p, T rhoe, T l) {
+  const bool ok = finite_(rho) && finite_(p) && finite_(rhoe) && (l == l);
+  return ok ? double(l) : 0.0;
+}
 
 // Primitive state at a face or a cell: rho, (u, v, w), e, p, h.
 template <typename T>
@@ -105,10 +123,21 @@ struct Stencil<3> {  // NODE (identity)
   static constexpr int LO = 0, RI = 1;
 };
 
-// MUSCL slope of cell c: phi(r) * dp with r = dnn(dm, dp).
+// MUSCL slope of cell c: phi(r) * dp with r = dnn(dm, dp), or (limiter 3)
+// the reference prototype's slope (demo/swirl_c_prototype.ipynb `muscl`,
+// cell 4): minmod of the central difference (v[c+1] - v[c-1]) / 4, the
+// forward and the backward difference, i.e. the smallest magnitude of the
+// three where all three have the same sign, else 0.
 template <typename T>
 __device__ __forceinline__ T muscl_slope(T vm1, T v0, T vp1, int limiter) {
   T dp = vp1 - v0, dm = v0 - vm1;
+  if (limiter == 3) {
+    const T c2 = (vp1 - vm1) * T(0.25);
+    const T m = min_(min_(abs_(c2), abs_(dp)), abs_(dm));
+    const bool up = c2 > T(0) && dp > T(0) && dm > T(0);
+    const bool down = c2 < T(0) && dp < T(0) && dm < T(0);
+    return up ? m : (down ? -m : T(0));
+  }
   T r = dnn(dm, dp);
   T phi;
   if (limiter == 0) {  // van Leer

@@ -700,7 +700,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
         T c = sqrt_(K<T>::gamma() * p / out[0]);
         T l = min_(min_(dx / (abs_(u) + c), dy / (abs_(v) + c)),
                    dz / (abs_(w) + c));
-        dtmin_local = fmin(dtmin_local, double(l));
+        dtmin_local = fmin(dtmin_local, cfl_limit_or_flag(out[0], p, out[4], l));
       }
     }
   }

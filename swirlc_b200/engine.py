@@ -27,7 +27,7 @@ from swirlc_b200.physics import constant
 _INTERP = {'WENO_5': nat.SWC_WENO5, 'WENO_3': nat.SWC_WENO3,
            'MUSCL': nat.SWC_MUSCL, 'NODE': nat.SWC_NODE}
 _LIMITER = {'van_leer': nat.SWC_LIM_VAN_LEER, 'mc': nat.SWC_LIM_MC,
-            'minmod': nat.SWC_LIM_MINMOD}
+            'minmod': nat.SWC_LIM_MINMOD, 'minmod3': nat.SWC_LIM_MINMOD3}
 _CELL_AVG = bc_types.BoundaryDictionaryType.CELL_AVERAGES.value
 _CELL_FACE = bc_types.BoundaryDictionaryType.CELL_FACES.value
 _CELL_FLUX = bc_types.BoundaryDictionaryType.INTERCELL_FLUXES.value
@@ -550,12 +550,24 @@ class Stepper:
         self._launch_step()
     torch.cuda.current_stream().wait_stream(side)
 
-  def step(self, n: int = 1) -> None:
+  def step(self, n: int = 1, check: bool = False) -> None:
+    """Advances n steps. With `check`, waits for them and raises
+    FloatingPointError if the new state holds a non-finite rho, p or rho_e
+    (or p/rho < 0), as flagged by the fused CFL reduction
+    (swc_clock_status)."""
     for _ in range(n):
       if self.graph is not None:
         self.graph.replay()
       else:
         self._launch_step()
+    if check:
+      self.check()
+
+  def check(self) -> None:
+    """Raises FloatingPointError if the last step left a non-finite or
+    unphysical state (waits for the current stream)."""
+    nat.check(nat.load().swc_clock_status(self.clock.data_ptr(),
+                                          nat.stream_ptr()), 'step')
 
   def time(self) -> float:
     return float(self.clock[0].item())

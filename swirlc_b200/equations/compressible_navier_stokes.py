@@ -108,3 +108,30 @@ def get_rhs_fn(replicas: np.ndarray, cfg, physics_models):
 
   rhs._swc_cache = cache  # lets rk3/rk2 run the fused in-place stages
   return rhs
+
+
+def _compute_physical_flux_1d(conservative: Dict, primitive: Dict,
+                              helper_var: Dict, dim: str,
+                              conservative_var_name: str):
+  """compressible_navier_stokes.py:338-427: the physical convective flux.
+
+  Mass flux rho*u_dim; momentum aligned with `dim`: rho*u_dim*u_dim + p (p_dyn
+  when the helper variable is present); energy: rho*u_dim*(e + p/rho) with the
+  full p; other conserved variables: rho*u_dim*phi. This is the flux the
+  fused stage and the pointwise Riemann kernel compute on the device; the
+  function is the reference's `flux_fn` argument of hll/hllc_convective_flux
+  and evaluates with torch operations on whatever tensors it is given.
+  """
+  p_updated = helper_var.get('p_dyn', primitive[types.P]) if helper_var \
+      else primitive[types.P]
+  var = types.conservative_to_primitive_name(conservative_var_name)
+  aligned_vel = types.VELOCITY[types.DIMS.index(dim)]
+  aligned_mom = types.primitive_to_conservative_name(aligned_vel)
+  m = conservative[aligned_mom]
+  if var == aligned_vel:
+    return m * primitive[aligned_vel] + p_updated
+  if var == types.E:
+    return m * (primitive[types.E] + primitive[types.P] / primitive[types.RHO])
+  if var == types.RHO:
+    return m
+  return m * primitive[var]

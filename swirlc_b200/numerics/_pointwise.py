@@ -78,6 +78,64 @@ def face_prims(prim: Dict, cons: Dict, scalars: Sequence[str],
   return [o.to(dt).reshape(-1).contiguous() for o in out]
 
 
+def check_flux_fn(flux_fn, names: Sequence[str]) -> None:
+  """Rejects a physical-flux function the fused kernel does not compute.
+
+  The CUDA Riemann kernel evaluates the reference's physical flux
+  (compressible_navier_stokes.py:338-427) itself. A `flux_fn` passed by the
+  caller (hll.py:45, hllc.py:42) is accepted when it is None or computes
+  that same flux; it is probed on a small float64 CPU state with
+  h = e + p / rho, per conserved variable and dimension. Any other flux
+  function raises NotImplementedError instead of being silently ignored.
+  """
+  if flux_fn is None:
+    return
+  from swirlc_b200.equations import compressible_navier_stokes as cns
+  if flux_fn is cns._compute_physical_flux_1d:  # pylint: disable=protected-access
+    return
+  g = torch.Generator().manual_seed(0)
+  r = lambda lo, hi: lo + (hi - lo) * torch.rand((2, 1, 1), generator=g,
+                                                  dtype=torch.float64)
+  prim = {types.RHO: r(0.5, 1.5), types.U: r(-1.0, 1.0),
+          types.V: r(-1.0, 1.0), types.W: r(-1.0, 1.0), types.P: r(0.5, 2.0)}
+  prim[types.E] = prim[types.P] / (0.4 * prim[types.RHO]) + r(0.0, 1.0)
+  prim[types.H] = prim[types.E] + prim[types.P] / prim[types.RHO]
+  cons = {types.RHO: prim[types.RHO]}
+  for n in names:
+    if n == types.RHO:
+      continue
+    pn = types.conservative_to_primitive_name(n)
+    if pn not in prim:
+      prim[pn] = r(0.0, 1.0)
+    cons[n] = prim[types.RHO] * prim[pn]
+  for dim in types.DIMS:
+    vel = types.VELOCITY[types.DIMS.index(dim)]
+    m = prim[types.RHO] * prim[vel]
+    for n in names:
+      pn = types.conservative_to_primitive_name(n)
+      if pn == types.RHO:
+        want = m
+      elif pn == vel:
+        want = m * prim[vel] + prim[types.P]
+      elif pn == types.E:
+        want = m * prim[types.H]
+      else:
+        want = m * prim[pn]
+      try:
+        got = torch.as_tensor(flux_fn(cons, prim, {}, dim, n),
+                              dtype=torch.float64)
+        ok = bool(torch.allclose(got, want, rtol=1e-12, atol=1e-12))
+      except Exception as e:  # a flux function that cannot run on the probe
+        raise NotImplementedError(
+            'flux_fn must compute the physical convective flux '
+            '(compressible_navier_stokes._compute_physical_flux_1d); the '
+            f'probe call failed: {e!r}') from e
+      if not ok:
+        raise NotImplementedError(
+            f'flux_fn differs from the physical convective flux for {n} '
+            f'along {dim}; the CUDA Riemann kernel computes only that flux.')
+
+
 def riemann_flux(riemann: int, conservative_neg, conservative_pos,
                  primitive_neg, primitive_pos, helper_var_neg, helper_var_pos,
                  dim: str, cfg, replica_id=0, replicas=None) -> Dict:

@@ -20,10 +20,13 @@ class FluxLimiterType(enum.Enum):
   MUSCL = 'mc'
   VAN_LEER = 'van_leer'
   MINMOD = 'minmod'
+  # The reference prototype's slope (demo/swirl_c_prototype.ipynb `muscl`):
+  # minmod of the central, forward and backward differences.
+  MINMOD3 = 'minmod3'
 
 
 _LIM = {'van_leer': nat.SWC_LIM_VAN_LEER, 'mc': nat.SWC_LIM_MC,
-        'minmod': nat.SWC_LIM_MINMOD}
+        'minmod': nat.SWC_LIM_MINMOD, 'minmod3': nat.SWC_LIM_MINMOD3}
 
 
 def weno(v, dim: str, k: int = 3):

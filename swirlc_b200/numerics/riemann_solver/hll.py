@@ -2,11 +2,12 @@
 
 hll_convective_flux evaluates hll.py:107-170 with the physical flux of
 compressible_navier_stokes.py:338-427 in one pointwise CUDA kernel
-(swc_riemann_flux). `flux_fn` is accepted for signature compatibility; the
-physical flux is the reference's own (_compute_physical_flux_1d).
+(swc_riemann_flux). `flux_fn` must be None or compute that physical flux
+(_compute_physical_flux_1d); any other function raises NotImplementedError.
 """
 
 from swirlc_b200 import _native as nat
+from swirlc_b200.common import types
 from swirlc_b200.numerics import _pointwise
 
 
@@ -15,7 +16,9 @@ def hll_convective_flux(replica_id, replicas, conservative_neg,
                         helper_var_neg, helper_var_pos, flux_fn, dim, cfg,
                         physics_models):
   """hll.py:36-175."""
-  del flux_fn, physics_models
+  del physics_models
+  _pointwise.check_flux_fn(flux_fn, list(getattr(
+      cfg, 'conservative_variable_names', types.BASE_CONSERVATIVE)))
   return _pointwise.riemann_flux(nat.SWC_HLL, conservative_neg,
                                  conservative_pos, primitive_neg,
                                  primitive_pos, helper_var_neg, helper_var_pos,

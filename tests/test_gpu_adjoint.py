@@ -178,6 +178,32 @@ def test_autograd_front_end_matches_reverse_sweep():
   assert float(nu.grad) == pytest.approx(nub2, rel=1e-12)
 
 
+def test_second_simulate_on_one_runner_is_refused_at_backward():
+  """A runner keeps the checkpoints of its latest run: the backward of an
+  earlier simulate() after a second one raises instead of reversing the
+  later trajectory; the later graph's backward still works and restores its
+  own nu."""
+  from swirlc_b200 import adjoint, configs
+  cfg, state = configs.kelvin_helmholtz(n=12, nu=1e-2, dtype=np.float64)
+  _, s, f = _setup(cfg, state)
+  run = adjoint.RunAdjoint(s, checkpoint_every=2)
+  nu1 = torch.tensor(1e-2, dtype=torch.float64, requires_grad=True)
+  nu2 = torch.tensor(3e-2, dtype=torch.float64, requires_grad=True)
+  x = [t.clone().requires_grad_(True) for t in f]
+  out1 = adjoint.simulate(run, x, [2e-3] * 3, nu1)
+  out2 = adjoint.simulate(run, x, [2e-3] * 3, nu2)
+  with pytest.raises(RuntimeError, match='run again'):
+    _loss(s, out1).backward()
+  s.scheme.nu = 0.5  # changed by the caller in between
+  _loss(s, out2).backward()
+  assert s.scheme.nu == pytest.approx(3e-2)
+  ref = adjoint.RunAdjoint(s, checkpoint_every=2)
+  s.scheme.nu = 3e-2
+  o = ref.run(f, [2e-3] * 3)
+  _, nub = ref.backward(_loss_grad(s, o))
+  assert float(nu2.grad) == pytest.approx(nub, rel=1e-9)
+
+
 def test_stored_stages_match_checkpointed_sweep():
   """checkpoint_every=0 keeps every stage state instead of recomputing:
   the same gradient (to summation order: the cotangents are accumulated

@@ -146,7 +146,7 @@ def test_linear_interpolation(dim):
 
 
 @pytest.mark.parametrize('scheme', ['weno5', 'weno3', 'mc', 'van_leer',
-                                    'minmod'])
+                                    'minmod', 'minmod3'])
 @pytest.mark.parametrize('dtype', [torch.float32, torch.float64])
 def test_reconstruction_matches_oracle(scheme, dtype):
   from swirlc_b200.numerics import interpolation
@@ -163,7 +163,8 @@ def test_reconstruction_matches_oracle(scheme, dtype):
     else:
       lt = {'mc': interpolation.FluxLimiterType.MUSCL,
             'van_leer': interpolation.FluxLimiterType.VAN_LEER,
-            'minmod': interpolation.FluxLimiterType.MINMOD}[scheme]
+            'minmod': interpolation.FluxLimiterType.MINMOD,
+            'minmod3': interpolation.FluxLimiterType.MINMOD3}[scheme]
       got, want = interpolation.flux_limiter(vt, dim, lt), orc.muscl(v, dim,
                                                                      scheme)
     tol = 2e-6 if dtype == torch.float32 else 1e-12

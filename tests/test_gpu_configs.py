@@ -1,7 +1,11 @@
 """GPU: full runs of the benchmark set-ups against the f32 oracle (the
 reference's float32 path restated) and against the same CUDA kernels in
 float64. Bar: relative L2 per conserved field <= 1e-5 after one step and
-<= 1e-3 after the full run."""
+<= 1e-3 after the full run.
+
+The oracle runs take their own CFL time steps (dt = CFL * cfl_dt_min of the
+oracle's state, the last step clamped to t_end), so the number of steps and
+every dt are checked against the device clock's, not borrowed from it."""
 
 import numpy as np
 import pytest
@@ -59,6 +63,35 @@ def _run_oracle(user_cfg, state, dts, dtype=np.float32):
   return outs
 
 
+def _run_oracle_cfl(user_cfg, state, max_steps, dtype=np.float32):
+  """Oracle run on its own CFL time steps; returns (outs, dts)."""
+  ocfg = _ocfg(user_cfg)
+  cfl, t_end = float(user_cfg['cfl']), float(user_cfg.get('t_end', 0.0))
+  s = {k: v.astype(dtype) for k, v in state.items()}
+  step = orc.rk3 if user_cfg.get('time_integration_scheme', 'rk3') == 'rk3' \
+      else orc.rk2
+  outs, dts, t = [], [], 0.0
+  for i in range(max_steps):
+    dt = cfl * orc.cfl_dt_min(s, ocfg)
+    if t_end > 0.0:
+      dt = min(dt, t_end - t)
+    s = step(s, dtype(dt), lambda u: orc.rhs(u, ocfg))
+    t += dt
+    dts.append(dt)
+    if i == 0:
+      outs.append(s)
+    if t_end > 0.0 and t >= t_end - 1e-12:
+      break
+  outs.append(s)
+  return outs, dts
+
+
+def _assert_dts(got, want, tol, what):
+  assert len(got) == len(want), f'{what}: {len(got)} vs {len(want)} steps'
+  rel = np.abs(np.asarray(got) - np.asarray(want)) / np.asarray(want)
+  assert rel.max() <= tol, f'{what}: dt rel err {rel.max():.3e}'
+
+
 def _assert_close(got, want, hw, tol, what, floor=None):
   """rel L2 per field <= tol, or <= 2x the float32 noise floor of that field
   (the reference path's own float32-vs-float64 error) when that is larger."""
@@ -74,7 +107,8 @@ def test_sod_to_t02_matches_oracle_and_fp64():
   hw = user_cfg['halo_width']
   g32, dts, st = _run_gpu(user_cfg, state, 1000, torch.float32, True)
   assert abs(st.time() - 0.2) < 1e-9
-  want = _run_oracle(user_cfg, state, dts)
+  want, odts = _run_oracle_cfl(user_cfg, state, 1000)
+  _assert_dts(dts, odts, 1e-5, 'sod dt sequence')
   _assert_close(g32[0], want[0], hw, 1e-5, 'sod step 1')
   _assert_close(g32[1], want[1], hw, 1e-3, f'sod t=0.2 ({len(dts)} steps)')
   g64, dts64, _ = _run_gpu(user_cfg, state, 1000, torch.float64, True)
@@ -98,7 +132,8 @@ def test_kelvin_helmholtz_matches_oracle():
   user_cfg, state = configs.kelvin_helmholtz(n=40, nu=1e-3)
   hw = user_cfg['halo_width']
   g32, dts, _ = _run_gpu(user_cfg, state, 6, torch.float32, True)
-  want = _run_oracle(user_cfg, state, dts)
+  want, odts = _run_oracle_cfl(user_cfg, state, 6)
+  _assert_dts(dts, odts, 1e-6, 'kh dt sequence')
   # rho_w is the 1e-3 noise field: its float32 floor is ~6e-5.
   _assert_close(g32[0], want[0], hw, 1e-5, 'kh step 1',
                 _floor(user_cfg, state, dts, hw))
@@ -112,7 +147,8 @@ def test_buoyant_bubble_matches_oracle():
   user_cfg, state = configs.buoyant_bubble(nx=24, ny=20, nz=16, lz=100.0)
   hw = user_cfg['halo_width']
   g32, dts, _ = _run_gpu(user_cfg, state, 5, torch.float32, True)
-  want = _run_oracle(user_cfg, state, dts)
+  want, odts = _run_oracle_cfl(user_cfg, state, 5)
+  _assert_dts(dts, odts, 1e-6, 'bubble dt sequence')
   _assert_close(g32[0], want[0], hw, 1e-5, 'bubble step 1',
                 _floor(user_cfg, state, dts, hw))
   # rho_u, rho_v ~ 1e-4 are perturbations of a hydrostatic p ~ 1e5: their

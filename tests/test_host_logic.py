@@ -153,6 +153,37 @@ def test_scheme_selection_errors():
   assert engine.interp_code(parameter.SwirlCParameters()) == nat.SWC_WENO5
 
 
+def test_riemann_flux_fn_is_checked_not_dropped():
+  """hll/hllc_convective_flux accept None, the reference's physical flux and
+  any function that computes it (the reference tests pass their own), and
+  raise for another flux instead of silently using the built-in one."""
+  from swirlc_b200.equations import compressible_navier_stokes as cns
+  from swirlc_b200.numerics import _pointwise
+  names = list(types.BASE_CONSERVATIVE) + ['rho_y']
+  _pointwise.check_flux_fn(None, names)
+  _pointwise.check_flux_fn(cns._compute_physical_flux_1d, names)
+
+  def from_enthalpy(cons, prim, helper, dim, name):
+    del cons, helper
+    var = types.conservative_to_primitive_name(name)
+    vel = types.VELOCITY[types.DIMS.index(dim)]
+    m = prim['rho'] * prim[vel]
+    if var == 'rho':
+      return m
+    if var == vel:
+      return m * prim[vel] + prim['p']
+    if var == 'e':
+      return m * prim['h']
+    return m * prim[var]
+
+  _pointwise.check_flux_fn(from_enthalpy, names)
+  with pytest.raises(NotImplementedError):
+    _pointwise.check_flux_fn(
+        lambda c, p, h, d, n: 2.0 * from_enthalpy(c, p, h, d, n), names)
+  with pytest.raises(NotImplementedError):
+    _pointwise.check_flux_fn(lambda c, p, h, d, n: p['no such key'], names)
+
+
 def test_names():
   assert types.primitive_to_conservative_name('u') == 'rho_u'
   assert types.conservative_to_primitive_name('rho_e') == 'e'
