@@ -342,6 +342,27 @@ int swc_wave_speeds(int64_t n, int32_t dtype, int32_t dim,
 int swc_stencil(const SwcGrid* grid, int32_t dtype, int32_t op, int32_t dim,
                 double h, const void* f, void* out, void* stream);
 
+/* Viscous terms on every face i-1/2 of a whole 3-D array (halo 0 grid, the
+ * spacings from grid->dx/dy/dz), from cell values q = {rho, u, v, w, p},
+ * computed with the fused stage's own face routine (so the values are bit
+ * for bit the viscous part of the stage's fluxes). Faces whose stencil
+ * leaves the array get 0. `what`:
+ *  SWC_VISC_FLUX   out[15]: diffusive flux of rho, rho_u, rho_v, rho_w,
+ *                  rho_e across x, y, z faces (out[d*5+k]);
+ *                  compressible_navier_stokes.py:618-707
+ *                  (_intercell_diffusive_flux); kappa = cp nu rho / pr.
+ *  SWC_VISC_STRAIN out[9]: strain rate S_ij on the j faces (out[i*3+j]),
+ *                  fluid.py:31-111 (reads u, v, w only).
+ *  SWC_VISC_STRESS out[9]: tau_ij = 2 rho_f nu S_ij with the face
+ *                  densities rho_face[j] given, diffusion.py:33-67.
+ *  SWC_VISC_HEAT   out[3]: heat flux -kappa_f dT/dx_j, T = p/(rho R),
+ *                  diffusion.py:76-109 (reads rho, p only). */
+enum { SWC_VISC_FLUX = 0, SWC_VISC_STRAIN = 1, SWC_VISC_STRESS = 2,
+       SWC_VISC_HEAT = 3 };
+int swc_viscous_terms(const SwcGrid* grid, int32_t dtype, int32_t what,
+                      const void* const* q, const void* const* rho_face,
+                      double nu, double pr, void* const* out, void* stream);
+
 /* Stage algebra for a user-supplied rhs function, elementwise over `n`
  * entries with the modes of swc_rk_stage (rk3.py:69-83, rk2.py:67-86):
  * EULER: out = uk + l*dt; CONVEX: out = u0*c0 + (uk + l*dt)*c1;

@@ -33,13 +33,15 @@ SWC_HLL, SWC_HLLC = 0, 1
 SWC_BC_PERIODIC, SWC_BC_DIRICHLET, SWC_BC_NEUMANN, SWC_BC_NONE = 0, 1, 2, 4
 SWC_OUT_RHS, SWC_OUT_EULER, SWC_OUT_CONVEX, SWC_OUT_AVERAGE = 0, 1, 2, 3
 SWC_MAX_FIELDS = 8
+SWC_VISC_FLUX, SWC_VISC_STRAIN, SWC_VISC_STRESS, SWC_VISC_HEAT = 0, 1, 2, 3
 
 # Every symbol include/swirlc_b200.h declares.
 EXPORTED = (
     'swc_abi_version', 'swc_last_error', 'swc_launch_count', 'swc_halo_fill',
     'swc_rk_stage', 'swc_cfl_reduce', 'swc_clock_begin_step',
     'swc_clock_end_step', 'swc_clock_status', 'swc_reconstruct', 'swc_riemann_flux',
-    'swc_wave_speeds', 'swc_stencil', 'swc_rk_combine', 'swc_rk_step',
+    'swc_wave_speeds', 'swc_stencil', 'swc_viscous_terms', 'swc_rk_combine',
+    'swc_rk_step',
     'swc_rk_step_noalloc', 'swc_batch_step', 'swc_rk_stage_ext',
     'swc_rk_stage_vjp',
 )
@@ -155,6 +157,8 @@ def load(require_cuda: bool = True) -> ctypes.CDLL:
                                       vp]
       lib.swc_stencil.argtypes = [ctypes.POINTER(SwcGrid), i32, i32, i32, dbl,
                                   vp, vp, vp]
+      lib.swc_viscous_terms.argtypes = [ctypes.POINTER(SwcGrid), i32, i32, pp,
+                                        pp, dbl, dbl, pp, vp]
       lib.swc_rk_combine.argtypes = [i64, i32, i32, dbl, dbl, vp, vp, vp, vp,
                                      vp, vp]
       lib.swc_rk_step.argtypes = [ctypes.POINTER(SwcGrid),
@@ -219,6 +223,14 @@ def ptr_array(tensors: Sequence[Optional[torch.Tensor]]):
   arr = (ctypes.c_void_p * max(1, len(tensors)))()
   for i, t in enumerate(tensors):
     arr[i] = None if t is None else t.data_ptr()
+  return arr
+
+
+def addr_array(addrs: Sequence[Optional[int]]):
+  """A void* array from raw device addresses (None for NULL)."""
+  arr = (ctypes.c_void_p * max(1, len(addrs)))()
+  for i, a in enumerate(addrs):
+    arr[i] = a
   return arr
 
 

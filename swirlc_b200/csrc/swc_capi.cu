@@ -306,6 +306,106 @@ static unsigned blocks_for(long long n, int threads = 256) {
   return (unsigned)std::max<long long>(1, std::min<long long>(b, 148 * 32));
 }
 
+// Viscous terms of every face i-1/2 of a whole array with the fused stage's
+// face routine: viscous_flux in the frame rotated so that the face normal is
+// axis 0, with the same launch-constant reciprocals, so a value here is bit
+// for bit the viscous part the stage kernel forms on that face.
+struct ViscArgs {
+  Geo3 g;
+  int what;
+  const void* q[5];   // rho, u, v, w, p
+  const void* rf[3];  // face densities (SWC_VISC_STRESS)
+  double h[3];
+  double nu, pr;
+  void* out[15];
+};
+
+template <typename T>
+__global__ void viscous_terms_kernel(const ViscArgs a) {
+  const Geo3& g = a.g;
+  const long long n = (long long)g.nxa * g.nya * g.nza;
+  const T* qv[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) qv[v] = static_cast<const T*>(a.q[v]);
+  const T h[3] = {T(a.h[0]), T(a.h[1]), T(a.h[2])};
+  const T rh[3] = {rcp_(h[0]), rcp_(h[1]), rcp_(h[2])};
+  const T r2h[3] = {rcp_(T(2) * h[0]), rcp_(T(2) * h[1]), rcp_(T(2) * h[2])};
+  const T nu = a.what == SWC_VISC_STRAIN ? T(0.5) : T(a.nu);
+  const T inv_pr = T(1.0 / a.pr);
+  const bool zero_vel = a.what == SWC_VISC_HEAT;
+  const bool cell_rho_p = a.what == SWC_VISC_FLUX || a.what == SWC_VISC_HEAT;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int x, y, z;
+    unflat(g, t, x, y, z);
+    const long long o = z * g.sz + x * g.sx + y;
+    const int c3[3] = {x, y, z};
+    const int ext[3] = {g.nxa, g.nya, g.nza};
+    const long long st[3] = {g.sx, 1, g.sz};
+#pragma unroll
+    for (int dn = 0; dn < 3; ++dn) {
+      const int t1 = dn == 0 ? 1 : 0, t2 = dn == 2 ? 1 : 2;
+      const bool ok = c3[dn] >= 1 && c3[t1] >= 1 && c3[t1] + 1 < ext[t1] &&
+                      c3[t2] >= 1 && c3[t2] + 1 < ext[t2];
+      T fo[5] = {T(0), T(0), T(0), T(0), T(0)};
+      if (ok) {
+        const long long ob = o, oa = o - st[dn];
+        const int vel[3] = {1 + dn, 1 + t1, 1 + t2};
+        T ua[3], ub[3], ga[3][3] = {}, gb[3][3] = {};
+        if (!zero_vel) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            ua[c] = qv[vel[c]][oa];
+            ub[c] = qv[vel[c]][ob];
+          }
+          const T i2t1 = T(2) * h[t1], i2t2 = T(2) * h[t2];
+          const long long s1 = st[t1], s2 = st[t2];
+          ga[1][1] = divk(qv[vel[1]][oa + s1] - qv[vel[1]][oa - s1], i2t1, r2h[t1]);
+          gb[1][1] = divk(qv[vel[1]][ob + s1] - qv[vel[1]][ob - s1], i2t1, r2h[t1]);
+          ga[1][0] = divk(qv[vel[0]][oa + s1] - qv[vel[0]][oa - s1], i2t1, r2h[t1]);
+          gb[1][0] = divk(qv[vel[0]][ob + s1] - qv[vel[0]][ob - s1], i2t1, r2h[t1]);
+          ga[2][2] = divk(qv[vel[2]][oa + s2] - qv[vel[2]][oa - s2], i2t2, r2h[t2]);
+          gb[2][2] = divk(qv[vel[2]][ob + s2] - qv[vel[2]][ob - s2], i2t2, r2h[t2]);
+          ga[2][0] = divk(qv[vel[0]][oa + s2] - qv[vel[0]][oa - s2], i2t2, r2h[t2]);
+          gb[2][0] = divk(qv[vel[0]][ob + s2] - qv[vel[0]][ob - s2], i2t2, r2h[t2]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) ua[c] = ub[c] = T(0);
+        }
+        T ra, rb;
+        if (a.what == SWC_VISC_STRAIN) {
+          ra = rb = T(1);
+        } else if (a.what == SWC_VISC_STRESS) {
+          ra = rb = static_cast<const T*>(a.rf[dn])[ob];
+        } else {
+          ra = qv[0][oa];
+          rb = qv[0][ob];
+        }
+        const T pa = cell_rho_p ? qv[4][oa] : T(1);
+        const T pb = cell_rho_p ? qv[4][ob] : T(1);
+        T f[5] = {T(0), T(0), T(0), T(0), T(0)};
+        viscous_flux<T, 0>(ra, rb, ua, ub, pa, pb, ga, gb, h[dn], rh[dn], nu,
+                           inv_pr, f);
+        // Back to (x, y, z) momentum order.
+        fo[1] = dn == 0 ? f[1] : f[2];
+        fo[2] = dn == 1 ? f[1] : (dn == 0 ? f[2] : f[3]);
+        fo[3] = dn == 2 ? f[1] : f[3];
+        fo[4] = f[4];
+      }
+      if (a.what == SWC_VISC_FLUX) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) static_cast<T*>(a.out[dn * 5 + k])[o] = fo[k];
+      } else if (a.what == SWC_VISC_HEAT) {
+        static_cast<T*>(a.out[dn])[o] = fo[4];
+      } else {
+        // tau_{c, dn} (strain: S_{c, dn}) = -(momentum flux c across dn).
+#pragma unroll
+        for (int c = 0; c < 3; ++c) static_cast<T*>(a.out[c * 3 + dn])[o] = -fo[1 + c];
+      }
+    }
+  }
+}
+
 }  // namespace swc
 
 using namespace swc;
@@ -823,6 +923,53 @@ int swc_wave_speeds(int64_t n, int32_t dtype, int32_t dim,
 #undef SWC_SP
   note_launch();
   return check_launch("wave_speeds");
+}
+
+int swc_viscous_terms(const SwcGrid* grid, int32_t dtype, int32_t what,
+                      const void* const* q, const void* const* rho_face,
+                      double nu, double pr, void* const* out, void* stream) {
+  int st = check_grid(grid);
+  if (st) return st;
+  if (!dtype_ok(dtype)) return fail(SWC_ERR_ARG, "bad dtype %d", dtype);
+  if (what < SWC_VISC_FLUX || what > SWC_VISC_HEAT)
+    return fail(SWC_ERR_ARG, "bad viscous quantity %d", what);
+  if (!q || !out) return fail(SWC_ERR_ARG, "NULL argument");
+  ViscArgs a;
+  memset(&a, 0, sizeof(a));
+  a.g = Geo3{grid->nx + 2 * grid->halo, grid->ny + 2 * grid->halo,
+             grid->nz + 2 * grid->halo, grid->sx, grid->sz};
+  a.what = what;
+  // Cell fields each quantity reads: rho and p (FLUX, HEAT), u, v, w (all
+  // but HEAT); face densities for STRESS.
+  const bool rp = what == SWC_VISC_FLUX || what == SWC_VISC_HEAT;
+  const bool vel = what != SWC_VISC_HEAT;
+  const bool need[5] = {rp, vel, vel, vel, rp};
+  for (int v = 0; v < 5; ++v) {
+    if (need[v] && !q[v]) return fail(SWC_ERR_ARG, "NULL cell field %d", v);
+    a.q[v] = q[v];
+  }
+  if (what == SWC_VISC_STRESS) {
+    if (!rho_face) return fail(SWC_ERR_ARG, "NULL face densities");
+    for (int d = 0; d < 3; ++d) {
+      if (!rho_face[d]) return fail(SWC_ERR_ARG, "NULL face density %d", d);
+      a.rf[d] = rho_face[d];
+    }
+  }
+  const int nout = what == SWC_VISC_FLUX ? 15 : (what == SWC_VISC_HEAT ? 3 : 9);
+  for (int k = 0; k < nout; ++k) {
+    if (!out[k]) return fail(SWC_ERR_ARG, "NULL output %d", k);
+    a.out[k] = out[k];
+  }
+  if (rp && !(pr > 0.0)) return fail(SWC_ERR_ARG, "Prandtl number must be > 0");
+  a.h[0] = grid->dx; a.h[1] = grid->dy; a.h[2] = grid->dz;
+  a.nu = nu;
+  a.pr = pr > 0.0 ? pr : 1.0;
+  long long n = (long long)a.g.nxa * a.g.nya * a.g.nza;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (dtype == SWC_F32) viscous_terms_kernel<float><<<blocks_for(n), 256, 0, s>>>(a);
+  else viscous_terms_kernel<double><<<blocks_for(n), 256, 0, s>>>(a);
+  note_launch();
+  return check_launch("viscous_terms");
 }
 
 int swc_stencil(const SwcGrid* grid, int32_t dtype, int32_t op, int32_t dim,

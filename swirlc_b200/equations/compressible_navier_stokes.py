@@ -135,3 +135,28 @@ def _compute_physical_flux_1d(conservative: Dict, primitive: Dict,
   if var == types.RHO:
     return m
   return m * primitive[var]
+
+
+def _intercell_diffusive_flux(primitive: Dict, cfg, physics_models) -> Dict:
+  """compressible_navier_stokes.py:618-707: the diffusive flux across every
+  face i-1/2 of every conserved variable: 0 for rho and transported
+  scalars, -tau_{i,dim} for rho_u_i, q_dim - u_f . tau_{.,dim} for rho_e;
+  computed by the fused stage's viscous face routine (swc_viscous_terms)."""
+  from swirlc_b200 import _native as nat
+  from swirlc_b200.numerics import _pointwise
+  tm = physics_models.transport_model
+  out = _pointwise.viscous_terms(nat.SWC_VISC_FLUX, primitive, cfg,
+                                 nu=tm.nu, pr=tm.pr)
+  names = list(getattr(cfg, 'conservative_variable_names',
+                       types.BASE_CONSERVATIVE))
+  ref = primitive[types.RHO]
+  base = dict(zip(types.BASE_CONSERVATIVE, range(5)))
+  res = {}
+  for d, dim in enumerate(types.DIMS):
+    res[dim] = {}
+    for name in names:
+      if name in base:
+        res[dim][name] = utils.like_input(out[d * 5 + base[name]], ref)
+      else:
+        res[dim][name] = utils.like_input(torch.zeros_like(out[d * 5]), ref)
+  return res

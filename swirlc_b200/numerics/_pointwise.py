@@ -216,3 +216,35 @@ def stencil(f, op: int, dim: str, h: float):
       dim_code(dim), float(h), t.data_ptr(), out.data_ptr(),
       nat.stream_ptr()), 'stencil')
   return utils.like_input(out, f)
+
+
+def viscous_terms(what: int, cell: Dict, cfg, rho_face=None, nu=None,
+                  pr=None) -> List[torch.Tensor]:
+  """swc_viscous_terms on whole 3-D arrays: cell values rho, u, v, w, p from
+  `cell` (names the quantity does not read may be absent), spacings from
+  cfg.dx/dy/dz, optional face densities [x, y, z]. Returns the output
+  arrays in the C-ABI's order."""
+  import ctypes
+  names = (types.RHO, types.U, types.V, types.W, types.P)
+  ref = next(cell[n] for n in names if n in cell)
+  t0 = cuda3d(ref)
+  dev, dtype = t0.device, t0.dtype
+  q = [cuda3d(cell[n], dev).to(dtype).contiguous() if n in cell else None
+       for n in names]
+  rf = None
+  if rho_face is not None:
+    rf = [cuda3d(r, dev).to(dtype).contiguous() for r in rho_face]
+  nz, nx, ny = t0.shape
+  grid = nat.SwcGrid(nx, ny, nz, 0, ny, ny * nx, float(cfg.dx), float(cfg.dy),
+                     float(cfg.dz))
+  nout = {nat.SWC_VISC_FLUX: 15, nat.SWC_VISC_HEAT: 3}.get(what, 9)
+  out = [torch.empty_like(t0) for _ in range(nout)]
+  if nu is None:
+    nu = cfg.transport_parameters['nu']
+  if pr is None:
+    pr = cfg.transport_parameters['pr']
+  nat.check(nat.load().swc_viscous_terms(
+      ctypes.byref(grid), nat.dtype_code(dtype), what, nat.ptr_array(q),
+      nat.ptr_array(rf) if rf is not None else None, float(nu), float(pr),
+      nat.ptr_array(out), nat.stream_ptr()), 'viscous terms')
+  return out
