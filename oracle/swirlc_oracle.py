@@ -54,6 +54,10 @@ BASE_CONSERVATIVE = (RHO, RHO_U, RHO_V, RHO_W, RHO_E)
 BASE_PRIMITIVES = (RHO, U, V, W, E)
 
 PERIODIC, DIRICHLET, NEUMANN, REFLECTIVE = 0, 1, 2, 3
+# Not a reference BC: the halo side is left as it is (a window cut out of a
+# larger grid whose halo rows hold the neighbouring cells, as in the C-ABI's
+# SWC_BC_NONE).
+NONE = 4
 
 
 def bc_kind(bc_type) -> int:
@@ -624,6 +628,8 @@ def exchange_halos(u, bc_dim: Dict[str, Any], hw: int) -> np.ndarray:
       continue
     for side in (0, 1):
       kind = bc_kind(sides[side][0])
+      if kind == NONE:
+        continue
       val = sides[side][1]
       if kind == DIRICHLET:
         for l in range(hw):

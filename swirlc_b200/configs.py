@@ -179,6 +179,28 @@ def buoyant_bubble(nx: int = 512, ny: int = 512, nz: int = 256, hw: int = 3,
   return cfg, _to_cons(rho, zero, zero, zero, p, pe=pe, dtype=dtype)
 
 
+def buoyant_bubble_reference_states(nx: int = 512, ny: int = 512,
+                                    nz: int = 256, hw: int = 3,
+                                    lz: float = 1.0e3,
+                                    dtype=np.float32) -> Dict[str, np.ndarray]:
+  """The helper states `p_ref`, `rho_ref` of the buoyant bubble: the
+  isothermal hydrostatic background (T0 = 300 K, p0 = 1e5) without the
+  bubble, on the same [nz+2h, nx+2h, ny+2h] arrays, as the reference demo
+  adds them (demo/buoyant_bubble/buoyant_bubble.py:321-323, 361-366). With
+  them the solver reconstructs p - p_ref and applies buoyancy to
+  rho - rho_ref (compressible_navier_stokes.py:299-335), which keeps the
+  horizontal momentum out of the float32 rounding of the 1e5 Pa balance."""
+  cfg = _base_cfg(nx, ny, nz, lz * nx / nz, lz * ny / nz, lz, hw)
+  zc = _halo_coords(cfg['z'], hw).astype(np.float64)
+  t0, p0 = 300.0, 1.0e5
+  p = p0 * np.exp(-constant.G * zc / (constant.R * t0))
+  rho = p / (constant.R * t0)
+  shape = (nz + 2 * hw, nx + 2 * hw, ny + 2 * hw)
+  ones = np.ones(shape)
+  return {'p_ref': (p[:, np.newaxis, np.newaxis] * ones).astype(dtype),
+          'rho_ref': (rho[:, np.newaxis, np.newaxis] * ones).astype(dtype)}
+
+
 def riemann_batch(members: int = 64, seed: int = 0, hw: int = 3):
   """64 quasi-1-D Riemann problems: nx log-uniform in [64, 4096],
   ny = nz in {4, 8, 16, 32}; rho in [0.1, 2], p in [0.1, 10], u in [-1, 1]
