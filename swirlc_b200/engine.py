@@ -408,6 +408,57 @@ class Solver:
         dtmin_out.data_ptr() if dtmin_out is not None else None,
         nat.stream_ptr()), 'rk stage')
 
+  def stage_box(self, uk, u0, uout, mode: int, box: Sequence[int],
+                c0: float = 0.0, c1: float = 0.0,
+                dt: Optional[torch.Tensor] = None,
+                dtmin_out: Optional[torch.Tensor] = None) -> None:
+    """The fused stage on the interior sub-box box = (x0, x1, y0, y1, z0, z1)
+    (interior cell indices, half-open) only. The same kernel runs on a grid
+    whose origin is the box's first cell, with the whole array's strides:
+    its stencils read the cells around the box, so a box at least
+    halo_width cells away from every face reads no halo cell, and the boxes
+    of a partition of the interior together give the whole stage bit for
+    bit. Not for the extended stage (its face and flux BCs act on the
+    grid's own faces)."""
+    if self.use_ext:
+      raise NotImplementedError('Sub-box stages need the plain fused stage.')
+    x0, x1, y0, y1, z0, z1 = (int(v) for v in box)
+    if not (0 <= x0 < x1 <= self.nx and 0 <= y0 < y1 <= self.ny and
+            0 <= z0 < z1 <= self.nz):
+      raise ValueError(f'Box {box} is not inside the {self.nx}x{self.ny}x'
+                       f'{self.nz} interior.')
+    g = nat.SwcGrid.from_buffer_copy(self.grid)
+    g.nx, g.ny, g.nz = x1 - x0, y1 - y0, z1 - z0
+    esz = torch.empty((), dtype=self.dtype).element_size()
+    off = (z0 * self.grid.sz + x0 * self.grid.sx + y0) * esz
+    sc = nat.SwcScheme.from_buffer_copy(self.scheme)
+    for i, o in enumerate((x0, y0, z0)):
+      if self.scheme.pe_axis[i]:
+        sc.pe_axis[i] = self.scheme.pe_axis[i] + o * esz
+    shift = lambda ts: nat.addr_array([t.data_ptr() + off for t in ts])
+    nat.check(nat.load().swc_rk_stage(
+        ctypes.byref(g), ctypes.byref(sc), shift(uk),
+        shift(u0) if u0 is not None else None, shift(uout), mode, float(c0),
+        float(c1), dt.data_ptr() if dt is not None else None,
+        dtmin_out.data_ptr() if dtmin_out is not None else None,
+        nat.stream_ptr()), 'rk stage (box)')
+
+  def split_boxes(self, margin_xy: int = 16):
+    """(inner, shell): the interior box whose stencils read no halo cell
+    (halo_width planes from the z faces, `margin_xy` cells -- one 16-cell
+    tile -- from the x and y faces) and the six boxes around it, or
+    (None, []) when the grid is too small to split."""
+    mz, m = self.hw, int(margin_xy)
+    nx, ny, nz = self.nx, self.ny, self.nz
+    if nx <= 2 * m or ny <= 2 * m or nz <= 2 * mz or m < self.hw:
+      return None, []
+    inner = (m, nx - m, m, ny - m, mz, nz - mz)
+    shell = [(0, nx, 0, ny, 0, mz), (0, nx, 0, ny, nz - mz, nz),
+             (0, m, 0, ny, mz, nz - mz), (nx - m, nx, 0, ny, mz, nz - mz),
+             (m, nx - m, 0, m, mz, nz - mz),
+             (m, nx - m, ny - m, ny, mz, nz - mz)]
+    return inner, shell
+
   def _helper_field(self, helper, name) -> torch.Tensor:
     t = utils.as_tensor3d(helper[name])
     if (tuple(t.shape) != self.shape or t.dtype != self.dtype or

@@ -1,4 +1,4 @@
-"""CPU (gloo, world size 2): halo exchange between the blocks of a decomposed
+"""CPU (gloo, world size 2 and 4): halo exchange between the blocks of a decomposed
 grid. After the exchange every block, halos and corners included, must equal
 its window of the single-grid halo fill done by the oracle on the whole grid
 (swirl_lm inplace_halo_exchange semantics as called at boundary.py:34-86)."""
@@ -41,6 +41,16 @@ def _case(name):
     bc['z'] = {0: (D, planes_lo), 1: (N, -0.5)}
     bc_u = dict(bc, z={0: (N, 0.0), 1: (D, 2.0)})
     return (1, 1, 2), (nz, nx, ny), [bc, bc_u, bc, bc, bc], [0, 1, 0, 0, 0]
+  if name == 'xy_2x2':
+    # Four blocks: x split with walls (Dirichlet per-layer planes low,
+    # Neumann high), y split and periodic, z periodic and not split; one
+    # field with its BC on the primitive.
+    nz, nx, ny = 4, 8, 10
+    planes = [rng.normal(size=(nz + 2 * HW, ny + 2 * HW)) for _ in range(HW)]
+    bc = {d: {0: (P,), 1: (P,)} for d in ('y', 'z')}
+    bc['x'] = {0: (D, planes), 1: (N, 0.75)}
+    bc_v = dict(bc, x={0: (N, -0.25), 1: (D, 3.0)})
+    return (2, 2, 1), (nz, nx, ny), [bc, bc, bc_v, bc, bc], [0, 0, 1, 0, 0]
   raise ValueError(name)
 
 
@@ -88,6 +98,9 @@ def _worker(rank, world, port, case, q):
       a[HW:-HW, HW:-HW, HW:-HW] = inner
       fields.append(torch.from_numpy(a))
     dims = ('x', 'y', 'z')
+    # Per-layer planes given for the whole grid, cut to this block's window.
+    local_bcs = [hx.localize_bc({'f': b}, replicas, rank, HW, (nz, nx, ny))['f']
+                 for b in bcs]
 
     def bc_fill(rid, fs, dim):
       d = dims[dim]
@@ -102,11 +115,11 @@ def _worker(rank, world, port, case, q):
               continue
             a = f.numpy()
             src = a if not via[i] else orc.divide_no_nan(a, fs[0].numpy())
-            sub = {d: bcs[i][d]}
+            sub = {d: local_bcs[i][d]}
             if layout.shape[dim] > 1 and not periodic[dim]:
               # Only this side is a wall: give the oracle both sides of it
               # and keep the side asked for.
-              sub = {d: {0: bcs[i][d][side], 1: bcs[i][d][side]}}
+              sub = {d: {0: local_bcs[i][d][side], 1: local_bcs[i][d][side]}}
             filled = orc.exchange_halos(src, sub, HW)
             if via[i]:
               filled = fs[0].numpy() * filled
@@ -133,18 +146,28 @@ def _worker(rank, world, port, case, q):
     q.put((rank, traceback.format_exc(), None))
 
 
-@pytest.mark.parametrize('case', ['x_walls', 'y_periodic', 'z_planes'])
-def test_two_block_exchange_matches_single_grid_fill(case):
+def _run(case, world):
   ctx = mp.get_context('spawn')
   q = ctx.Queue()
   port = _free_port()
-  procs = [ctx.Process(target=_worker, args=(r, 2, port, case, q))
-           for r in range(2)]
+  procs = [ctx.Process(target=_worker, args=(r, world, port, case, q))
+           for r in range(world)]
   for p in procs:
     p.start()
   results = [q.get(timeout=240) for _ in procs]
   for p in procs:
     p.join(timeout=60)
+  return results
+
+
+@pytest.mark.parametrize('case,world', [('x_walls', 2), ('y_periodic', 2),
+                                        ('z_planes', 2), ('xy_2x2', 4)])
+def test_block_exchange_matches_single_grid_fill(case, world):
+  """Two blocks, and a 2x2x1 split over four ranks (walls with per-layer
+  Dirichlet planes and a primitive BC on one split dim, periodic wrap on the
+  other): every block, halos and corners included, equals its window of the
+  single-grid fill."""
+  results = _run(case, world)
   via = _case(case)[3]
   for rank, errs, m in results:
     assert isinstance(errs, dict), errs
