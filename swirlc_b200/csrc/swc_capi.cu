@@ -345,8 +345,11 @@ __global__ void viscous_terms_kernel(const ViscArgs a) {
 #pragma unroll
     for (int dn = 0; dn < 3; ++dn) {
       const int t1 = dn == 0 ? 1 : 0, t2 = dn == 2 ? 1 : 2;
-      const bool ok = c3[dn] >= 1 && c3[t1] >= 1 && c3[t1] + 1 < ext[t1] &&
-                      c3[t2] >= 1 && c3[t2] + 1 < ext[t2];
+      // The heat flux reads only the two cells of the face; the other
+      // quantities also read their tangential neighbours.
+      const bool ok = c3[dn] >= 1 &&
+                      (zero_vel || (c3[t1] >= 1 && c3[t1] + 1 < ext[t1] &&
+                                    c3[t2] >= 1 && c3[t2] + 1 < ext[t2]));
       T fo[5] = {T(0), T(0), T(0), T(0), T(0)};
       if (ok) {
         const long long ob = o, oa = o - st[dn];

@@ -7,8 +7,6 @@ reduction then reports it through the device clock, and
 FloatingPointError (C status SWC_ERR_NONFINITE from swc_clock_status).
 """
 
-import ctypes
-
 import numpy as np
 import pytest
 import torch
@@ -72,7 +70,6 @@ def test_cfl_reduce_flags_a_bad_initial_state():
   nat.check(nat.load().swc_clock_status(clock.data_ptr(), nat.stream_ptr()))
   with pytest.raises(ValueError):
     nat.check(nat.load().swc_clock_status(None, nat.stream_ptr()))
-  del ctypes
 
 
 def test_batch_names_the_bad_member():
