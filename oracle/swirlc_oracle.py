@@ -14,11 +14,14 @@ Parity status:
   * Riemann solvers, physical flux, divergence, thermodynamics, transport,
     diffusion, gravity, halo fill, RK3/RK2 and the stencils are pinned by the
     reference's own known-answer tests (ported in tests/).
-  * WENO5/WENO3/MUSCL reconstruction lives in the un-vendored, unpinned
-    dependency `swirl-lm` (pyproject.toml:32, bare git URL, no commit). Its
-    arithmetic is restated from the reference's own NumPy prototype
-    (demo/swirl_c_prototype.ipynb, `weno5`, cell 4), re-indexed to the
-    production convention "index i holds face i-1/2". Parity unpinned.
+  * WENO5 (`weno(k=3)`), the prototype's MUSCL slope (`muscl(limiter=
+    'minmod3')`), HLL, RK3 and the CFL rule are pinned to outputs of the
+    reference's own NumPy prototype (demo/swirl_c_prototype.ipynb, cells 4,
+    5, 11, 16), executed by tests/golden/make_prototype_fixtures.py; the two
+    reconstructions agree bit for bit. The production reference calls its
+    WENO and flux limiter in the un-vendored `swirl-lm` (pyproject.toml:32,
+    bare git URL, no commit): the 'mc', 'van_leer' and 'minmod' limiters and
+    WENO3 are restatements of the published schemes, parity unpinned.
 """
 
 from __future__ import annotations

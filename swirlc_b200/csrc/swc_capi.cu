@@ -647,7 +647,12 @@ int swc_rk_stage(const SwcGrid* grid, const SwcScheme* sc,
     return fail(SWC_ERR_UNSUPPORTED,
                 "transported scalars go through swc_rk_stage_ext");
   StageArgs a;
-  int st = stage_args(grid, sc, 5, sc && sc->dtype == SWC_F32 ? 2 : 1, 16, uk,
+  // Resident CTAs per SM of the plain stage kernel (its launch bounds):
+  // three for the inviscid single-precision MUSCL stage, two for the other
+  // single-precision ones, one in double precision.
+  const int per_sm = !sc || sc->dtype != SWC_F32 ? 1
+                     : (sc->interp == SWC_MUSCL && !sc->diffusion ? 3 : 2);
+  int st = stage_args(grid, sc, 5, per_sm, 16, uk,
                       u0, uout, mode, c0, c1, dt, dtmin_out, a);
   if (st) return st;
   const int visc = sc->diffusion ? 1 : 0;

@@ -138,18 +138,21 @@ __device__ __forceinline__ T muscl_slope(T vm1, T v0, T vp1, int limiter) {
     const bool down = c2 < T(0) && dp < T(0) && dm < T(0);
     return up ? m : (down ? -m : T(0));
   }
+  if (limiter == 0) {  // van Leer
+    // phi(r) dp = (r + |r|) / (1 + |r|) dp with r = dm / dp is, in exact
+    // arithmetic, the harmonic mean 2 dm dp / (dm + dp) where dm and dp have
+    // the same sign and 0 elsewhere (dp = 0 or dm = 0 included, as
+    // divide_no_nan gives r = 0 there). It is formed as
+    // 2 dm * (dp / (dm + dp)): one division instead of two, no ratio r and
+    // no product that can overflow (dp / (dm + dp) lies in (0, 1]), so
+    // extreme ratios beside subnormal values (double precision keeps them)
+    // need no special case.
+    const bool same = (dm > T(0) && dp > T(0)) || (dm < T(0) && dp < T(0));
+    return same ? (dm + dm) * (dp / (dm + dp)) : T(0);
+  }
   T r = dnn(dm, dp);
   T phi;
-  if (limiter == 0) {  // van Leer
-    // From |r| >= 2^54 (2^25 in single precision) 1 + |r| rounds to |r| and
-    // the formula gives exactly 2 (r > 0) or 0 (r < 0); those values are
-    // taken directly there, which also covers ratios where r + |r|
-    // overflows or r is infinite (dp subnormal under dm: double precision
-    // keeps subnormals), for which the formula gives inf or NaN.
-    T a = abs_(r);
-    const T big = sizeof(T) == 8 ? T(18014398509481984.0) : T(33554432.0);
-    phi = a >= big ? (r > T(0) ? T(2) : T(0)) : (r + a) / (T(1) + a);
-  } else if (limiter == 1) {  // monotonized central
+  if (limiter == 1) {  // monotonized central
     phi = max_(T(0), min_(min_(T(2) * r, T(0.5) * (T(1) + r)), T(2)));
   } else {  // minmod
     phi = max_(T(0), min_(r, T(1)));

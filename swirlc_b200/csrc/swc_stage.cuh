@@ -725,8 +725,15 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
   }
 }
 
+// Resident CTAs per SM the register budget is set for: the inviscid MUSCL
+// stage in single precision is light enough (shared memory 70 KB) for three.
+template <typename T, int SCHEME, bool VISC>
+constexpr int stage_min_blocks() {
+  return sizeof(T) == 4 ? ((SCHEME == 2 && !VISC) ? 3 : 2) : 1;
+}
+
 template <typename T, int SCHEME, int RIEMANN, bool VISC, int TY, int TX>
-__global__ void __launch_bounds__(TY* TX, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(TY* TX, (stage_min_blocks<T, SCHEME, VISC>()))
     stage_kernel(const StageArgs a) {
   stage_body<T, SCHEME, RIEMANN, VISC, TY, TX>(a, nullptr, blockIdx.x * TY,
                                                blockIdx.y * TX, blockIdx.z);
