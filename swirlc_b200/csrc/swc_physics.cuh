@@ -123,11 +123,13 @@ struct Stencil<3> {  // NODE (identity)
   static constexpr int LO = 0, RI = 1;
 };
 
-// MUSCL slope of cell c: phi(r) * dp with r = dnn(dm, dp), or (limiter 3)
-// the reference prototype's slope (demo/swirl_c_prototype.ipynb `muscl`,
-// cell 4): minmod of the central difference (v[c+1] - v[c-1]) / 4, the
-// forward and the backward difference, i.e. the smallest magnitude of the
-// three where all three have the same sign, else 0.
+// MUSCL slope of cell c for the monotonized-central (1) and minmod (2)
+// limiters: phi(r) * dp with r = dnn(dm, dp); or (limiter 3) the reference
+// prototype's slope (demo/swirl_c_prototype.ipynb `muscl`, cell 4): minmod
+// of the central difference (v[c+1] - v[c-1]) / 4, the forward and the
+// backward difference, i.e. the smallest magnitude of the three where all
+// three have the same sign, else 0. The van Leer limiter (0) is formed lane
+// by lane in muscl_slope_v.
 template <typename T>
 __device__ __forceinline__ T muscl_slope(T vm1, T v0, T vp1, int limiter) {
   T dp = vp1 - v0, dm = v0 - vm1;
@@ -137,18 +139,6 @@ __device__ __forceinline__ T muscl_slope(T vm1, T v0, T vp1, int limiter) {
     const bool up = c2 > T(0) && dp > T(0) && dm > T(0);
     const bool down = c2 < T(0) && dp < T(0) && dm < T(0);
     return up ? m : (down ? -m : T(0));
-  }
-  if (limiter == 0) {  // van Leer
-    // phi(r) dp = (r + |r|) / (1 + |r|) dp with r = dm / dp is, in exact
-    // arithmetic, the harmonic mean 2 dm dp / (dm + dp) where dm and dp have
-    // the same sign and 0 elsewhere (dp = 0 or dm = 0 included, as
-    // divide_no_nan gives r = 0 there). It is formed as
-    // 2 dm * (dp / (dm + dp)): one division instead of two, no ratio r and
-    // no product that can overflow (dp / (dm + dp) lies in (0, 1]), so
-    // extreme ratios beside subnormal values (double precision keeps them)
-    // need no special case.
-    const bool same = (dm > T(0) && dp > T(0)) || (dm < T(0) && dp < T(0));
-    return same ? (dm + dm) * (dp / (dm + dp)) : T(0);
   }
   T r = dnn(dm, dp);
   T phi;
@@ -209,6 +199,10 @@ struct One<float> {
   static __device__ __forceinline__ V add(V a, V b) { return __fadd_rn(a, b); }
   static __device__ __forceinline__ V sub(V a, V b) { return __fsub_rn(a, b); }
   static __device__ __forceinline__ V rcp(V a) { return 1.0f / a; }
+  // a / b as a times the reciprocal of b (what the fast-math quotient is).
+  static __device__ __forceinline__ V div(V a, V b) { return __fmul_rn(a, 1.0f / b); }
+  // x where p > 0, else 0.
+  static __device__ __forceinline__ V sel_pos(V p, V x) { return p > 0.0f ? x : 0.0f; }
   template <class F>
   static __device__ __forceinline__ V map3(F f, V a, V b, V c) { return f(a, b, c); }
 };
@@ -222,6 +216,8 @@ struct One<double> {
   static __device__ __forceinline__ V add(V a, V b) { return __dadd_rn(a, b); }
   static __device__ __forceinline__ V sub(V a, V b) { return __dsub_rn(a, b); }
   static __device__ __forceinline__ V rcp(V a) { return 1.0 / a; }
+  static __device__ __forceinline__ V div(V a, V b) { return __ddiv_rn(a, b); }
+  static __device__ __forceinline__ V sel_pos(V p, V x) { return p > 0.0 ? x : 0.0; }
   template <class F>
   static __device__ __forceinline__ V map3(F f, V a, V b, V c) { return f(a, b, c); }
 };
@@ -239,6 +235,10 @@ struct Two<float> {
   // a - b, rounded once (b * -1 is exact).
   static __device__ __forceinline__ V sub(V a, V b) { return __ffma2_rn(b, splat(-1.0f), a); }
   static __device__ __forceinline__ V rcp(V a) { return make_float2(1.0f / a.x, 1.0f / a.y); }
+  static __device__ __forceinline__ V div(V a, V b) { return __fmul2_rn(a, rcp(b)); }
+  static __device__ __forceinline__ V sel_pos(V p, V x) {
+    return make_float2(p.x > 0.0f ? x.x : 0.0f, p.y > 0.0f ? x.y : 0.0f);
+  }
   template <class F>
   static __device__ __forceinline__ V map3(F f, V a, V b, V c) {
     return make_float2(f(a.x, b.x, c.x), f(a.y, b.y, c.y));
@@ -263,6 +263,12 @@ struct Two<double> {
     return make_double2(__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y));
   }
   static __device__ __forceinline__ V rcp(V a) { return make_double2(1.0 / a.x, 1.0 / a.y); }
+  static __device__ __forceinline__ V div(V a, V b) {
+    return make_double2(__ddiv_rn(a.x, b.x), __ddiv_rn(a.y, b.y));
+  }
+  static __device__ __forceinline__ V sel_pos(V p, V x) {
+    return make_double2(p.x > 0.0 ? x.x : 0.0, p.y > 0.0 ? x.y : 0.0);
+  }
   template <class F>
   static __device__ __forceinline__ V map3(F f, V a, V b, V c) {
     return make_double2(f(a.x, b.x, c.x), f(a.y, b.y, c.y));
@@ -411,6 +417,19 @@ __device__ __forceinline__ typename O::V muscl_slope_v(typename O::V vm1,
                                                        typename O::V vp1,
                                                        int limiter) {
   using S = typename O::S;
+  if (limiter == 0) {
+    // van Leer: phi(r) dp = (r + |r|) / (1 + |r|) dp with r = dm / dp is, in
+    // exact arithmetic, the harmonic mean 2 dm dp / (dm + dp) where dm and
+    // dp have the same sign (dm dp > 0) and 0 elsewhere (dp = 0 or dm = 0
+    // included, as divide_no_nan gives r = 0 there). It is formed as
+    // 2 dm * (dp / (dm + dp)): one quotient instead of two, no ratio r and
+    // no product that can overflow (dp / (dm + dp) lies in (0, 1]), so
+    // extreme ratios beside subnormal values (double precision keeps them)
+    // need no special case; every lane op is a paired one where O pairs.
+    const typename O::V dp = O::sub(vp1, v0), dm = O::sub(v0, vm1);
+    const typename O::V q = O::div(dp, O::add(dm, dp));
+    return O::sel_pos(O::mul(dm, dp), O::mul(O::add(dm, dm), q));
+  }
   return O::map3([limiter](S a, S b, S c) { return muscl_slope(a, b, c, limiter); },
                  vm1, v0, vp1);
 }
