@@ -696,8 +696,9 @@ def update_faces(c_neg, c_pos, p_neg, p_pos, cfg):
   """boundary.py:340-461 with _face_boundary_update_1d (:239-337), one
   replica: face values on the planes between halo and interior; as in the
   reference, the other member of the (conservative, primitive) pair is then
-  recomputed over the whole array. A density face BC is not restated (the
-  reference then drops p and h from the face primitives)."""
+  recomputed over the whole array. A density face BC is applied first and
+  rebuilds the face primitives from the conservative values (:279-293), which
+  drops p and h, as the reference does."""
   bcf = (cfgget(cfg, 'bc') or {}).get('cell_faces')
   if not bcf:
     return
@@ -708,12 +709,17 @@ def update_faces(c_neg, c_pos, p_neg, p_pos, cfg):
       bc1 = _interface_bc(bcf, d, side)
       if not bc1:
         continue
-      if RHO in bc1:
-        raise NotImplementedError('density face BC')
-      for cons, prim in ((c_neg[d], p_neg[d]), (c_pos[d], p_pos[d])):
+      for cd, pd in ((c_neg, p_neg), (c_pos, p_pos)):
+        cons = cd[d]
         n = cons[RHO].shape[ax] - 2 * hw
         idx = hw if side == 0 else hw + n
+        if RHO in bc1:
+          _set_plane(cons[RHO], ax, idx, _plane_value(bc1[RHO], cons[RHO]))
+          pd[d] = conservative_to_primitive(cons)
+        prim = pd[d]
         for name, val in bc1.items():
+          if name == RHO:
+            continue
           if name in cons:
             pname = conservative_to_primitive_name(name)
             _set_plane(cons[name], ax, idx, _plane_value(val, cons[name]))
@@ -742,7 +748,19 @@ def update_fluxes(flux, cfg, flux_type: str):
 
 
 def rhs(cons: Dict[str, np.ndarray], cfg, helper: Optional[Dict] = None,
-        interp_fn=None, apply_bc=True, pe=None) -> Dict[str, np.ndarray]:
+        interp_fn=None, apply_bc=True, pe=None, conv_flux_fn=None,
+        diff_flux_fn=None, grad_fn=None, source_fn=None
+        ) -> Dict[str, np.ndarray]:
+  """compressible_navier_stokes.py:68-268.
+
+  The keyword hooks stand where the reference's own tests patch it:
+  `interp_fn` for swirl_lm's weno, `apply_bc=False` for
+  update_conservative_cell_averages, `conv_flux_fn(c_neg, c_pos, p_neg,
+  p_pos)` for _intercell_convective_flux (returns {dim: {var: flux}}),
+  `diff_flux_fn(prim)` for _intercell_diffusive_flux, `grad_fn(f, h, dim)`
+  for gradient.forward_1 in the divergence, and `source_fn(cons)` for
+  physics_models.source_function (added to the gravity source).
+  """
   helper = dict(helper or {})
   if apply_bc:
     cons = update_conservative_cell_averages(dict(cons), cfg)
@@ -782,11 +800,16 @@ def rhs(cons: Dict[str, np.ndarray], cfg, helper: Optional[Dict] = None,
     ffn = hllc_flux
   else:
     raise ValueError(f'"{scheme}" is not implemented as a "numeric_flux_scheme".')
-  flux = {d: ffn(c_neg[d], c_pos[d], p_neg[d], p_pos[d], h_neg[d], h_pos[d], d,
-                 names, pe) for d in DIMS}
+  if conv_flux_fn is not None:
+    flux = conv_flux_fn(c_neg, c_pos, p_neg, p_pos)
+  else:
+    flux = {d: ffn(c_neg[d], c_pos[d], p_neg[d], p_pos[d], h_neg[d],
+                   h_pos[d], d, names, pe) for d in DIMS}
   flux = update_fluxes(flux, cfg, 'convective')
   if cfgget(cfg, 'include_diffusion', False):
-    fd = update_fluxes(diffusive_flux(prim, cfg, names), cfg, 'diffusive')
+    dflux = (diff_flux_fn(prim) if diff_flux_fn is not None
+             else diffusive_flux(prim, cfg, names))
+    fd = update_fluxes(dflux, cfg, 'diffusive')
     for d in DIMS:
       for k in names:
         flux[d][k] = flux[d][k] + fd[d][k]
@@ -804,10 +827,15 @@ def rhs(cons: Dict[str, np.ndarray], cfg, helper: Optional[Dict] = None,
     for i, d in enumerate(DIMS):
       if MOMENTUM[i] in mask:
         source[MOMENTUM[i]] = source[MOMENTUM[i]] + d_rho * G * g[d]
+  if source_fn is not None:
+    extra = source_fn(cons)
+    for k in names:
+      source[k] = source[k] + extra[k]
   delta = {'x': cfg.dx, 'y': cfg.dy, 'z': cfg.dz}
+  grad = grad_fn or forward_1
   for k in names:
     for d in DIMS:
-      source[k] = source[k] - forward_1(flux[d][k], delta[d], d)
+      source[k] = source[k] - grad(flux[d][k], delta[d], d)
   return source
 
 

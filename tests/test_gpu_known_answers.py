@@ -197,3 +197,35 @@ def test_intercell_flux_standing_shock(dim, solver):
     for k in NAMES6:
       np.testing.assert_allclose(_np(got[k])[WIN], expected[fd][k][WIN],
                                  rtol=1e-6, atol=1e-6, err_msg=f'{fd} {k}')
+
+
+@pytest.mark.parametrize('kind', ['convective', 'total'])
+def test_fused_rhs_intercell_flux_bcs(kind):
+  """compressible_navier_stokes_test.py:1484-1826 through the fused
+  extended stage: a uniform moving state with Dirichlet flux BCs on the x
+  boundary faces (identity face values, the real HLL flux). The halo
+  (left as given in the reference test) is filled here with zero-gradient
+  x and periodic y, z conditions, which for the uniform state leave it as
+  it is. Interior cells only (the stage writes no halo cells)."""
+  from swirlc_b200.boundary import bc_types
+  from swirlc_b200.equations import compressible_navier_stokes as cns
+  from tests import test_oracle_rhs_mocked_cases as mc
+  cons, ocfg, expected = mc.flux_bc_case(kind)
+  B = bc_types.BoundaryCondition
+  conv = lambda t: (None, None) if t[0] is None else (B.DIRICHLET, t[1])
+  fluxes = {k: {d: {s: conv(v) for s, v in sides.items()}
+                for d, sides in spec.items()}
+            for k, spec in ocfg.bc['intercell_fluxes'][kind].items()}
+  per = {0: (B.PERIODIC,), 1: (B.PERIODIC,)}
+  cells = {k: {'x': {0: (B.NEUMANN, 0.0), 1: (B.NEUMANN, 0.0)}, 'y': per,
+               'z': per} for k in NAMES6}
+  cfg = _cfg(dx=1.0, dy=1.0, dz=1.0, interpolation_scheme='NODE',
+             numeric_flux_scheme='HLL', conservative_variable_names=NAMES6,
+             bc={'cell_averages': cells, 'intercell_fluxes': {kind: fluxes}})
+  rhs = cns.get_rhs_fn(np.array([[[0]]]), cfg, _pm(cfg))
+  out = rhs(0, _dev(cons), {})
+  inner = (slice(3, -3),) * 3
+  for k, want in expected.items():
+    np.testing.assert_allclose(_np(out[k])[inner], want[inner], rtol=1e-9,
+                               atol=1e-9 * max(np.abs(want).max(), 1.0),
+                               err_msg=k)
