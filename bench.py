@@ -365,7 +365,8 @@ def run_decomposed(args):
   del state
   mine = {rank: blocks[rank]} if world > 1 else blocks
   ds = decomposition.DecomposedStepper(
-      user_cfg, mine, transport='dist' if world > 1 else 'local')
+      user_cfg, mine, transport='dist' if world > 1 else 'local',
+      overlap=not args.no_overlap)
   ds.step(args.warmup)
   torch.cuda.synchronize()
 
@@ -1053,6 +1054,9 @@ def main():
   ap.add_argument('--decomposed', default='',
                   help='cx,cy,cz: one --n^3 domain split into blocks (one '
                        'per rank under torchrun, else all in this process)')
+  ap.add_argument('--no-overlap', action='store_true',
+                  help='--decomposed: halo update before each stage instead '
+                       'of behind the inner boxes')
   ap.add_argument('--profile-steps', type=int, default=0,
                   help='only run this many eager RK3 steps of the workload '
                        '(a small, untimed command for ncu captures)')
