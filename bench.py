@@ -366,7 +366,7 @@ def run_decomposed(args):
   mine = {rank: blocks[rank]} if world > 1 else blocks
   ds = decomposition.DecomposedStepper(
       user_cfg, mine, transport='dist' if world > 1 else 'local',
-      overlap=not args.no_overlap)
+      overlap=False if args.no_overlap else True)
   ds.step(args.warmup)
   torch.cuda.synchronize()
 

@@ -11,7 +11,8 @@ A decomposed run reproduces the single-grid run bit for bit: the
 `mesh_local` halo-coordinate rule (utils.py:58-89) gives an inner block's
 halo cells its neighbours' coordinates.
 
-With `overlap` (the default where every block is large enough), each stage
+With `overlap` (the default for the distributed transport, where every
+block is large enough), each stage
 runs in two parts: the halo update (boundary conditions and the transfers
 between blocks) is issued on a separate CUDA stream while the stage kernel
 advances each block's inner box, whose stencils read no halo cell; the
@@ -86,12 +87,17 @@ class DecomposedStepper:
     dt, cfl, t_end, scheme: as `engine.Stepper`.
     overlap: hide the halo update behind the inner boxes' stage work (used
       only where every block splits, see `engine.Solver.split_boxes`).
+      Default: on for the distributed transport, off for the local one,
+      whose device-to-device copies compete with the stage kernel on the
+      same GPU (KH 256^3 in 2x2x1 blocks on one B200: 8.15 ms per step
+      overlapped, 7.74 ms not).
   """
 
   def __init__(self, cfg, states: Dict[int, Dict], dtype=torch.float32,
                transport: str = 'local', dt: Optional[float] = None,
                cfl: Optional[float] = None, t_end: Optional[float] = None,
-               scheme: str = 'rk3', device=None, overlap: bool = True):
+               scheme: str = 'rk3', device=None,
+               overlap: Optional[bool] = None):
     if not isinstance(cfg, parameter.SwirlCParameters):
       cfg = parameter.SwirlCParameters(cfg)
     if scheme not in ('rk3', 'rk2'):
@@ -147,6 +153,8 @@ class DecomposedStepper:
     if mcfl > 0.0:
       self.exchange.min_all([c[2:3] for c in self.clocks])
     self.boxes = [s.split_boxes() for s in self.solvers]
+    if overlap is None:
+      overlap = transport == 'dist'
     self.overlap = bool(overlap) and all(
         not s.use_ext and b[0] is not None
         for s, b in zip(self.solvers, self.boxes))
