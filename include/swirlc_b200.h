@@ -257,8 +257,9 @@ typedef struct SwcBatchMember {
 int swc_batch_step(const SwcScheme* scheme, int32_t order, int32_t nmembers,
                    const SwcBatchMember* members, void* stream);
 
-/* Reverse mode of one fused stage for WENO5 + HLLC (+ viscous), no
- * transported scalars, on the halo-filled state `uk` of that stage. On the
+/* Reverse mode of one fused stage for WENO5 or MUSCL (any SWC_LIM_*
+ * limiter) with HLL or HLLC (+ viscous), no transported scalars, on the
+ * halo-filled state `uk` of that stage (halo width >= 3). On the
  * interior cells
  *   vout = alpha*lam + c1*x1 + c2*x2 + beta * H^T J_L(H uk)^T lam,
  * (x1, x2 may be NULL; H: halo fill with `bcs`), halos of vout set to 0,

@@ -33,7 +33,8 @@ class RunAdjoint:
   """A forward run with checkpoints and its reverse sweep for one solver.
 
   Args:
-    solver: an `engine.Solver` (WENO5 + HLLC, optionally viscous).
+    solver: an `engine.Solver` (WENO5 or MUSCL, HLL or HLLC, optionally
+      viscous; no transported scalars).
     checkpoint_every: steps between stored states; 0 keeps every step's
       stage states during the forward run instead (no recomputation in the
       backward sweep; memory: steps x 3 states of the fields).

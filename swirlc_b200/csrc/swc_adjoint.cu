@@ -1,8 +1,9 @@
-// Reverse mode (vector-Jacobian product) of one fused RK stage for WENO5 +
-// HLLC (+ viscous) on a halo-filled state: the discrete adjoint used to
-// differentiate whole runs (gradients with respect to the initial state and
-// to the kinematic viscosity nu). For a stage out = A*u0 + B*(uk + dt*L(uk))
-// the caller needs lambda_out^T dout/duk = B*lambda + B*dt*H^T J_L^T lambda,
+// Reverse mode (vector-Jacobian product) of one fused RK stage for WENO5 or
+// MUSCL with HLL or HLLC (+ viscous) on a halo-filled state: the discrete
+// adjoint used to differentiate whole runs (gradients with respect to the
+// initial state and to the kinematic viscosity nu). For a stage
+// out = A*u0 + B*(uk + dt*L(uk)) the caller needs
+// lambda_out^T dout/duk = B*lambda + B*dt*H^T J_L^T lambda,
 // where H is the halo fill; swc_rk_stage_vjp computes
 //   vout = beta * H^T J_L(H uk)^T lambda   (beta = B*dt),
 //   nu_bar += beta * lambda . dL/dnu.
@@ -139,32 +140,122 @@ __device__ __forceinline__ T dsqrt(T root, T bar) {
   return root > T(0) ? bar / (T(2) * root) : T(0);
 }
 
+// Forward values of hll_speeds<T, 0> that its reverse needs.
+template <typename T>
+struct SpeedsFwd {
+  T cl, cr, rl, rr, inv, nu_[3], ru[3], nh, rc, s_l, s_r;
+  bool lmin_a, rmax_a;  // which candidate min / max picked
+};
+template <typename T>
+__device__ __forceinline__ SpeedsFwd<T> speeds_fwd(const Prim<T>& l,
+                                                   const Prim<T>& r, T pe) {
+  const T gam = K<T>::gamma(), gm1 = K<T>::gm1();
+  SpeedsFwd<T> w;
+  w.cl = sqrt_(gam * l.p / l.r);
+  w.cr = sqrt_(gam * r.p / r.r);
+  w.rl = sqrt_(l.r);
+  w.rr = sqrt_(r.r);
+  const T den = w.rl + w.rr;
+  w.inv = den == T(0) ? T(0) : T(1) / den;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    w.nu_[i] = w.rl * l.u[i] + w.rr * r.u[i];
+    w.ru[i] = w.nu_[i] * w.inv;
+  }
+  w.nh = w.rl * l.h + w.rr * r.h;
+  const T rh = w.nh * w.inv;
+  const T hs = rh - T(0.5) * (w.ru[0] * w.ru[0] + w.ru[1] * w.ru[1] +
+                              w.ru[2] * w.ru[2]) - pe;
+  w.rc = sqrt_(gm1 * hs);
+  const T sla = l.u[0] - w.cl, slb = w.ru[0] - w.rc;
+  const T sra = r.u[0] + w.cr, srb = w.ru[0] + w.rc;
+  w.lmin_a = sla <= slb;
+  w.rmax_a = sra >= srb;
+  w.s_l = w.lmin_a ? sla : slb;
+  w.s_r = w.rmax_a ? sra : srb;
+  return w;
+}
+
+// Reverse of speeds_fwd for the cotangents slb_ of s_l and srb_ of s_r.
+template <typename T>
+__device__ __forceinline__ void speeds_vjp(const SpeedsFwd<T>& w,
+                                           const Prim<T>& l, const Prim<T>& r,
+                                           T slb_, T srb_, PrimBar<T>& lb,
+                                           PrimBar<T>& rb) {
+  const T gam = K<T>::gamma(), gm1 = K<T>::gm1();
+  T clb = T(0), crb = T(0), rcb = T(0), rub[3] = {T(0), T(0), T(0)};
+  if (w.lmin_a) {
+    lb.u[0] += slb_;
+    clb += -slb_;
+  } else {
+    rub[0] += slb_;
+    rcb += -slb_;
+  }
+  if (w.rmax_a) {
+    rb.u[0] += srb_;
+    crb += srb_;
+  } else {
+    rub[0] += srb_;
+    rcb += srb_;
+  }
+  const T hsb = dsqrt(w.rc, rcb) * gm1;
+  const T rhb = hsb;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) rub[i] += -hsb * w.ru[i];
+  T rlb = T(0), rrb = T(0), invb = T(0);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    rlb += rub[i] * l.u[i] * w.inv;
+    lb.u[i] += rub[i] * w.rl * w.inv;
+    rrb += rub[i] * r.u[i] * w.inv;
+    rb.u[i] += rub[i] * w.rr * w.inv;
+    invb += rub[i] * w.nu_[i];
+  }
+  rlb += rhb * l.h * w.inv;
+  lb.h += rhb * w.rl * w.inv;
+  rrb += rhb * r.h * w.inv;
+  rb.h += rhb * w.rr * w.inv;
+  invb += rhb * w.nh;
+  const T denb = -invb * w.inv * w.inv;
+  rlb += denb;
+  rrb += denb;
+  lb.r += dsqrt(w.rl, rlb);
+  rb.r += dsqrt(w.rr, rrb);
+  // c = sqrt(gamma p / rho)
+  const T cl2b = dsqrt(w.cl, clb), cr2b = dsqrt(w.cr, crb);
+  lb.p += cl2b * gam / l.r;
+  lb.r += -cl2b * gam * l.p / (l.r * l.r);
+  rb.p += cr2b * gam / r.r;
+  rb.r += -cr2b * gam * r.p / (r.r * r.r);
+}
+
+// Reverse of physical_flux<T, 0>(q, q.p) for the flux cotangent gb.
+template <typename T>
+__device__ __forceinline__ void phys_vjp(const Prim<T>& q, const T* gb,
+                                         PrimBar<T>& qb) {
+  const T m = q.r * q.u[0];
+  const T eh = q.e + q.p / q.r;
+  const T mb = gb[0] + gb[1] * q.u[0] + gb[2] * q.u[1] + gb[3] * q.u[2] +
+               gb[4] * eh;
+  qb.u[0] += gb[1] * m;
+  qb.u[1] += gb[2] * m;
+  qb.u[2] += gb[3] * m;
+  qb.p += gb[1] + gb[4] * m / q.r;
+  qb.e += gb[4] * m;
+  qb.r += -gb[4] * m * q.p / (q.r * q.r);
+  qb.r += mb * q.u[0];
+  qb.u[0] += mb * q.r;
+}
+
 // Reverse of hllc_flux<T, 0> with p_dyn = p (no helper states): fb is the
 // cotangent of the 5 flux components (rotated momentum order).
 template <typename T>
 __device__ __forceinline__ void hllc_vjp(const Prim<T>& l, const Prim<T>& r,
                                          T pe, const T* fb, PrimBar<T>& lb,
                                          PrimBar<T>& rb) {
-  const T gam = K<T>::gamma(), gm1 = K<T>::gm1();
   // ---- forward
-  const T cl = sqrt_(gam * l.p / l.r), cr = sqrt_(gam * r.p / r.r);
-  const T rl = sqrt_(l.r), rr = sqrt_(r.r);
-  const T den = rl + rr;
-  const T inv = den == T(0) ? T(0) : T(1) / den;
-  T nu_[3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) nu_[i] = rl * l.u[i] + rr * r.u[i];
-  T ru[3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) ru[i] = nu_[i] * inv;
-  const T nh = rl * l.h + rr * r.h;
-  const T rh = nh * inv;
-  const T hs = rh - T(0.5) * (ru[0] * ru[0] + ru[1] * ru[1] + ru[2] * ru[2]) - pe;
-  const T rc = sqrt_(gm1 * hs);
-  const T sla = l.u[0] - cl, slb = ru[0] - rc;
-  const T sra = r.u[0] + cr, srb = ru[0] + rc;
-  const bool lmin_a = sla <= slb, rmax_a = sra >= srb;
-  const T s_l = lmin_a ? sla : slb, s_r = rmax_a ? sra : srb;
+  const SpeedsFwd<T> w = speeds_fwd(l, r, pe);
+  const T s_l = w.s_l, s_r = w.s_r;
   const T vl = l.u[0], vr = r.u[0];
   const T num = (r.p - l.p) + l.r * vl * (s_l - vl) - r.r * vr * (s_r - vr);
   const T dd = l.r * (s_l - vl) - r.r * (s_r - vr);
@@ -180,17 +271,7 @@ __device__ __forceinline__ void hllc_vjp(const Prim<T>& l, const Prim<T>& r,
   PrimBar<T>& qb = left ? lb : rb;
   const T s_k = left ? s_l : s_r;
   // ---- reverse: physical flux of side k
-  const T m = q.r * q.u[0];
-  const T eh = q.e + q.p / q.r;
-  T mb = fb[0] + fb[1] * q.u[0] + fb[2] * q.u[1] + fb[3] * q.u[2] + fb[4] * eh;
-  qb.u[0] += fb[1] * m;
-  qb.u[1] += fb[2] * m;
-  qb.u[2] += fb[3] * m;
-  qb.p += fb[1] + fb[4] * m / q.r;
-  qb.e += fb[4] * m;
-  qb.r += -fb[4] * m * q.p / (q.r * q.r);
-  qb.r += mb * q.u[0];
-  qb.u[0] += mb * q.r;
+  phys_vjp(q, fb, qb);
   T skb = T(0), smb = T(0);
   if (star) {
     const T v = q.u[0];
@@ -256,50 +337,187 @@ __device__ __forceinline__ void hllc_vjp(const Prim<T>& l, const Prim<T>& r,
     rb.u[0] += -numb * r.r * (s_r - T(2) * vr) + ddb * r.r;
     srb_ += -numb * r.r * vr - ddb * r.r;
   }
-  T clb = T(0), crb = T(0), rcb = T(0), rub[3] = {T(0), T(0), T(0)};
-  if (lmin_a) {
-    lb.u[0] += slb_;
-    clb += -slb_;
-  } else {
-    rub[0] += slb_;
-    rcb += -slb_;
-  }
-  if (rmax_a) {
-    rb.u[0] += srb_;
-    crb += srb_;
-  } else {
-    rub[0] += srb_;
-    rcb += srb_;
-  }
-  const T hsb = dsqrt(rc, rcb) * gm1;
-  const T rhb = hsb;
+  speeds_vjp(w, l, r, slb_, srb_, lb, rb);
+}
+
+// sign(x) with sign(0) = 0: the derivative of |x| on the branch taken.
+template <typename T>
+__device__ __forceinline__ T sgn0(T x) {
+  return x > T(0) ? T(1) : (x < T(0) ? T(-1) : T(0));
+}
+
+// Reverse of hll_flux<T, 0> with p_dyn = p (no helper states):
+// F = t1 F_R + t2 F_L - t3 (U_R - U_L) with t1 = dnn(min(s_r, 0) -
+// min(s_l, 0), s_r - s_l), t2 = 1 - t1, t3 = dnn(s_r |s_l| - s_l |s_r|,
+// 2 (s_r - s_l)) (hll.py:107-170); fb as in hllc_vjp.
+template <typename T>
+__device__ __forceinline__ void hll_vjp(const Prim<T>& l, const Prim<T>& r,
+                                        T pe, const T* fb, PrimBar<T>& lb,
+                                        PrimBar<T>& rb) {
+  // ---- forward
+  const SpeedsFwd<T> w = speeds_fwd(l, r, pe);
+  const T s_l = w.s_l, s_r = w.s_r;
+  const T ds = s_r - s_l;
+  const T A = min_(s_r, T(0)) - min_(s_l, T(0));
+  const T B = s_r * abs_(s_l) - s_l * abs_(s_r);
+  const T t1 = ds == T(0) ? T(0) : A / ds;
+  const T t3 = ds == T(0) ? T(0) : B / (T(2) * ds);
+  const T t2 = T(1) - t1;
+  const T m_l = l.r * l.u[0], m_r = r.r * r.u[0];
+  const T fl[5] = {m_l, m_l * l.u[0] + l.p, m_l * l.u[1], m_l * l.u[2],
+                   m_l * (l.e + l.p / l.r)};
+  const T fr[5] = {m_r, m_r * r.u[0] + r.p, m_r * r.u[1], m_r * r.u[2],
+                   m_r * (r.e + r.p / r.r)};
+  const T ul[5] = {l.r, l.r * l.u[0], l.r * l.u[1], l.r * l.u[2], l.r * l.e};
+  const T ur[5] = {r.r, r.r * r.u[0], r.r * r.u[1], r.r * r.u[2], r.r * r.e};
+  // ---- reverse
+  T t1b = T(0), t3b = T(0), flb[5], frb[5], db[5];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) rub[i] += -hsb * ru[i];
-  T rlb = T(0), rrb = T(0), invb = T(0);
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    rlb += rub[i] * l.u[i] * inv;
-    lb.u[i] += rub[i] * rl * inv;
-    rrb += rub[i] * r.u[i] * inv;
-    rb.u[i] += rub[i] * rr * inv;
-    invb += rub[i] * nu_[i];
+  for (int k = 0; k < 5; ++k) {
+    t1b += fb[k] * (fr[k] - fl[k]);  // t2 = 1 - t1
+    t3b -= fb[k] * (ur[k] - ul[k]);
+    frb[k] = fb[k] * t1;
+    flb[k] = fb[k] * t2;
+    db[k] = -fb[k] * t3;  // cotangent of U_R - U_L
   }
-  rlb += rhb * l.h * inv;
-  lb.h += rhb * rl * inv;
-  rrb += rhb * r.h * inv;
-  rb.h += rhb * rr * inv;
-  invb += rhb * nh;
-  const T denb = -invb * inv * inv;
-  rlb += denb;
-  rrb += denb;
-  lb.r += dsqrt(rl, rlb);
-  rb.r += dsqrt(rr, rrb);
-  // c = sqrt(gamma p / rho)
-  const T cl2b = dsqrt(cl, clb), cr2b = dsqrt(cr, crb);
-  lb.p += cl2b * gam / l.r;
-  lb.r += -cl2b * gam * l.p / (l.r * l.r);
-  rb.p += cr2b * gam / r.r;
-  rb.r += -cr2b * gam * r.p / (r.r * r.r);
+  phys_vjp(l, flb, lb);
+  phys_vjp(r, frb, rb);
+  // U = (rho, rho u, rho e)
+  auto cons_vjp = [](const Prim<T>& q, T sgn, const T* ub, PrimBar<T>& qb) {
+    qb.r += sgn * (ub[0] + ub[1] * q.u[0] + ub[2] * q.u[1] + ub[3] * q.u[2] +
+                   ub[4] * q.e);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) qb.u[i] += sgn * ub[1 + i] * q.r;
+    qb.e += sgn * ub[4] * q.r;
+  };
+  cons_vjp(r, T(1), db, rb);
+  cons_vjp(l, T(-1), db, lb);
+  T slb_ = T(0), srb_ = T(0);
+  if (ds != T(0)) {
+    const T Ab = t1b / ds, Bb = t3b / (T(2) * ds);
+    const T dsb = -(t1b * A) / (ds * ds) - (t3b * B) / (T(2) * ds * ds);
+    if (s_r < T(0)) srb_ += Ab;
+    if (s_l < T(0)) slb_ -= Ab;
+    srb_ += Bb * (abs_(s_l) - s_l * sgn0(s_r));
+    slb_ += Bb * (s_r * sgn0(s_l) - abs_(s_r));
+    srb_ += dsb;
+    slb_ -= dsb;
+  }
+  speeds_vjp(w, l, r, slb_, srb_, lb, rb);
+}
+
+// Reverse of muscl_slope (limiters 1-3) and of muscl_slope_v's van Leer
+// slope (0): adds sb * d slope / d(vm1, v0, vp1) to bm1, b0, bp1, on the
+// branch the forward takes.
+template <typename T>
+__device__ __forceinline__ void muscl_slope_vjp(T vm1, T v0, T vp1,
+                                                int limiter, T sb, T& bm1,
+                                                T& b0, T& bp1) {
+  const T dp = vp1 - v0, dm = v0 - vm1;
+  T gdm = T(0), gdp = T(0);  // d slope / d dm, d slope / d dp
+  if (limiter == 0) {
+    // 2 dm dp / (dm + dp) where dm dp > 0, else 0.
+    if (dm * dp > T(0)) {
+      const T is = T(1) / (dm + dp);
+      gdm = T(2) * dp * dp * is * is;
+      gdp = T(2) * dm * dm * is * is;
+    }
+  } else if (limiter == 3) {
+    // Smallest magnitude of c2 = (vp1 - vm1) / 4, dp and dm where all
+    // three share a sign.
+    const T c2 = (vp1 - vm1) * T(0.25);
+    const bool up = c2 > T(0) && dp > T(0) && dm > T(0);
+    const bool down = c2 < T(0) && dp < T(0) && dm < T(0);
+    if (up || down) {
+      const T ac = abs_(c2), ap = abs_(dp), am = abs_(dm);
+      if (ac <= ap && ac <= am) {
+        bp1 += T(0.25) * sb;
+        bm1 -= T(0.25) * sb;
+        return;
+      }
+      if (ap <= am) gdp = T(1);
+      else gdm = T(1);
+    }
+  } else if (dp != T(0)) {
+    // phi(r) dp with r = dm / dp: d/d dm = phi'(r), d/d dp = phi - phi' r.
+    const T r = dm / dp;
+    T m, dmr;
+    if (limiter == 1) {  // max(0, min(min(2 r, (1 + r) / 2), 2))
+      const T a = T(2) * r, b = T(0.5) * (T(1) + r);
+      m = a <= b ? a : b;
+      dmr = a <= b ? T(2) : T(0.5);
+      if (!(m <= T(2))) {
+        m = T(2);
+        dmr = T(0);
+      }
+    } else {  // minmod: max(0, min(r, 1))
+      m = r <= T(1) ? r : T(1);
+      dmr = r <= T(1) ? T(1) : T(0);
+    }
+    const T phi = m > T(0) ? m : T(0);
+    const T dphi = m > T(0) ? dmr : T(0);
+    gdm = dphi;
+    gdp = phi - dphi * r;
+  }
+  // dp = vp1 - v0, dm = v0 - vm1. (dp = 0 gives r = 0 and phi(0) = 0 for
+  // both ratio limiters, so the slope and its derivative vanish there.)
+  bp1 += sb * gdp;
+  b0 += sb * (gdm - gdp);
+  bm1 -= sb * gdm;
+}
+
+// Reverse of recon_cell<2> (MUSCL) on one lane: right = v0 + slope / 2,
+// left = v0 - slope / 2 with cotangents rb, lb.
+template <typename T>
+__device__ __forceinline__ void muscl_cell_vjp(T vm1, T v0, T vp1, T rb, T lb,
+                                               int limiter, T& bm1, T& b0,
+                                               T& bp1) {
+  b0 += rb + lb;
+  muscl_slope_vjp(vm1, v0, vp1, limiter, T(0.5) * (rb - lb), bm1, b0, bp1);
+}
+__device__ __forceinline__ void muscl_cell_vjp(float2 vm1, float2 v0,
+                                               float2 vp1, float2 rb,
+                                               float2 lb, int limiter,
+                                               float2& bm1, float2& b0,
+                                               float2& bp1) {
+  muscl_cell_vjp(vm1.x, v0.x, vp1.x, rb.x, lb.x, limiter, bm1.x, b0.x, bp1.x);
+  muscl_cell_vjp(vm1.y, v0.y, vp1.y, rb.y, lb.y, limiter, bm1.y, b0.y, bp1.y);
+}
+__device__ __forceinline__ void muscl_cell_vjp(double2 vm1, double2 v0,
+                                               double2 vp1, double2 rb,
+                                               double2 lb, int limiter,
+                                               double2& bm1, double2& b0,
+                                               double2& bp1) {
+  muscl_cell_vjp(vm1.x, v0.x, vp1.x, rb.x, lb.x, limiter, bm1.x, b0.x, bp1.x);
+  muscl_cell_vjp(vm1.y, v0.y, vp1.y, rb.y, lb.y, limiter, bm1.y, b0.y, bp1.y);
+}
+
+// Both face values of the cell v[2] from the five cells v[0..4] =
+// v[c-2 .. c+2] of the face kernel's window (MUSCL uses v[1..3]).
+template <int SCHEME, class O>
+__device__ __forceinline__ void recon5(const typename O::V* v, int limiter,
+                                       typename O::V& left,
+                                       typename O::V& right) {
+  if constexpr (SCHEME == 0) recon_cell<0, O>(v, limiter, left, right);
+  else recon_cell<2, O>(v + 1, limiter, left, right);
+}
+// Reverse of recon5: vb[k] += d right / dv[k] * rb + d left / dv[k] * lb.
+template <int SCHEME, class O>
+__device__ __forceinline__ void cell_vjp5(const typename O::V* v,
+                                          typename O::V rb, typename O::V lb,
+                                          int limiter, typename O::V* vb) {
+  if constexpr (SCHEME == 0) weno5_cell_vjp_v<O>(v, rb, lb, vb);
+  else muscl_cell_vjp(v[1], v[2], v[3], rb, lb, limiter, vb[1], vb[2], vb[3]);
+}
+
+// Reverse of the Riemann flux RIEMANN (0 HLL, 1 HLLC).
+template <int RIEMANN, typename T>
+__device__ __forceinline__ void riemann_vjp(const Prim<T>& l,
+                                            const Prim<T>& r, T pe,
+                                            const T* fb, PrimBar<T>& lb,
+                                            PrimBar<T>& rb) {
+  if constexpr (RIEMANN == 0) hll_vjp<T>(l, r, pe, fb, lb, rb);
+  else hllc_vjp<T>(l, r, pe, fb, lb, rb);
 }
 
 // Reverse of viscous_flux<T, 0> for the cotangent fb[1..4]. gab/gbb are the
@@ -410,6 +628,7 @@ struct VjpArgs {
   double g[3];
   double* nu_bar;
   int seg;  // faces per thread along a line
+  int limiter;  // MUSCL limiter (SWC_LIM_*)
   // vout = alpha*lam + c1*x1 + c2*x2 + beta*H^T J^T lam on the interior.
   double alpha, c1, c2;
   const void* x1[5];
@@ -520,7 +739,7 @@ __global__ void __launch_bounds__(256) vjp_prim_kernel(const VjpArgs a) {
 #define SWC_VJP_FACE_MINB 1
 #endif
 
-template <typename T, int D>
+template <typename T, int D, int SCHEME, int RIEMANN>
 __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
     vjp_face_kernel(const VjpArgs a) {
   const int h = a.h;
@@ -627,11 +846,11 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
     for (int v = 0; v < 3; ++v) {
       const V2 s5[5] = {sw[0][v], sw[1][v], sw[2][v], sw[3][v], sw[4][v]};
       V2 lv;
-      recon_cell<0, O2>(s5, 0, lv, qn[v]);
+      recon5<SCHEME, O2>(s5, a.limiter, lv, qn[v]);
     }
     const T s5[5] = {swh[0], swh[1], swh[2], swh[3], swh[4]};
     T lv;
-    recon_cell<0, O1>(s5, 0, lv, qnh);
+    recon5<SCHEME, O1>(s5, a.limiter, lv, qnh);
   }
   lam_at(active ? i0 - 1 : -1, la);
   const T scale = T(a.beta) / hd;
@@ -709,11 +928,11 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
       const V2 s5[5] = {sw[1][v], sw[2][v], sw[3][v], sw[4][v], sw[5][v]};
-      recon_cell<0, O2>(s5, 0, lv[v], rn[v]);
+      recon5<SCHEME, O2>(s5, a.limiter, lv[v], rn[v]);
     }
     {
       const T s5[5] = {swh[1], swh[2], swh[3], swh[4], swh[5]};
-      recon_cell<0, O1>(s5, 0, lvh, rnh);
+      recon5<SCHEME, O1>(s5, a.limiter, lvh, rnh);
     }
     Prim<T> ql, qr;
     ql.r = qn[0].x; ql.u[0] = qn[1].x; ql.u[1] = qn[1].y; ql.u[2] = qn[2].x;
@@ -731,7 +950,7 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
     PrimBar<T> lbar, rbar;
     lbar.zero();
     rbar.zero();
-    hllc_vjp<T>(ql, qr, pe, fr, lbar, rbar);
+    riemann_vjp<RIEMANN, T>(ql, qr, pe, fr, lbar, rbar);
     if (a.visc) {
       // Cells a = i-1 (window 2) and b = i (window 3).
       // Cell a: rho, u, p (rotated frame) from the pairs.
@@ -775,14 +994,14 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
       for (int v = 0; v < 3; ++v) {
         const V2 s5[5] = {sw[0][v], sw[1][v], sw[2][v], sw[3][v], sw[4][v]};
         V2 acc[5] = {ab[0][v], ab[1][v], ab[2][v], ab[3][v], ab[4][v]};
-        weno5_cell_vjp_v<O2>(s5, cr[v], cl[v], acc);
+        cell_vjp5<SCHEME, O2>(s5, cr[v], cl[v], a.limiter, acc);
 #pragma unroll
         for (int k = 0; k < 5; ++k) ab[k][v] = acc[k];
       }
       {
         const T s5[5] = {swh[0], swh[1], swh[2], swh[3], swh[4]};
         T acc[5] = {abh[0], abh[1], abh[2], abh[3], abh[4]};
-        weno5_cell_vjp_v<O1>(s5, lbar.h, clh, acc);
+        cell_vjp5<SCHEME, O1>(s5, lbar.h, clh, a.limiter, acc);
 #pragma unroll
         for (int k = 0; k < 5; ++k) abh[k] = acc[k];
       }
@@ -820,14 +1039,14 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
     for (int v = 0; v < 3; ++v) {
       const V2 s5[5] = {sw[0][v], sw[1][v], sw[2][v], sw[3][v], sw[4][v]};
       V2 acc[5] = {ab[0][v], ab[1][v], ab[2][v], ab[3][v], ab[4][v]};
-      weno5_cell_vjp_v<O2>(s5, z2, cl[v], acc);
+      cell_vjp5<SCHEME, O2>(s5, z2, cl[v], a.limiter, acc);
 #pragma unroll
       for (int k = 0; k < 5; ++k) ab[k][v] = acc[k];
     }
     {
       const T s5[5] = {swh[0], swh[1], swh[2], swh[3], swh[4]};
       T acc[5] = {abh[0], abh[1], abh[2], abh[3], abh[4]};
-      weno5_cell_vjp_v<O1>(s5, T(0), clh, acc);
+      cell_vjp5<SCHEME, O1>(s5, T(0), clh, a.limiter, acc);
 #pragma unroll
       for (int k = 0; k < 5; ++k) abh[k] = acc[k];
     }
@@ -1040,26 +1259,33 @@ __global__ void __launch_bounds__(256) vjp_halo_kernel(const VjpHalo a) {
   }
 }
 
+// Above 48 KB of dynamic shared memory a kernel must opt in: done on the
+// first call per dtype (whatever the scheme), which the header asks callers
+// to make outside stream capture.
 template <typename T>
+int vjp_smem_opt_in() {
+  static bool smem_set = false;
+  if (smem_set) return SWC_OK;
+  const size_t tile_bytes = sizeof(T) * TT * (TT + 1);
+  if (cudaFuncSetAttribute(vjp_prim_kernel<T>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(kPrimTiles * tile_bytes)) != cudaSuccess ||
+      cudaFuncSetAttribute(vjp_cell_kernel<T>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(kCellTiles * tile_bytes)) != cudaSuccess)
+    return record_error(SWC_ERR_LAUNCH, "stage vjp: shared memory opt-in");
+  smem_set = true;
+  return SWC_OK;
+}
+
+template <typename T, int SCHEME, int RIEMANN>
 int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
   const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h, nza = a.nz + 2 * a.h;
   const dim3 tgrid((nya + TT - 1) / TT, (nxa + TT - 1) / TT, nza);
   const dim3 tblock(TT, 8);
   const size_t tile_bytes = sizeof(T) * TT * (TT + 1);
-  // Above 48 KB of dynamic shared memory a kernel must opt in: done on the
-  // first call per dtype, which the header asks callers to make outside
-  // stream capture.
-  static bool smem_set = false;
-  if (!smem_set) {
-    if (cudaFuncSetAttribute(vjp_prim_kernel<T>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(kPrimTiles * tile_bytes)) != cudaSuccess ||
-        cudaFuncSetAttribute(vjp_cell_kernel<T>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(kCellTiles * tile_bytes)) != cudaSuccess)
-      return record_error(SWC_ERR_LAUNCH, "stage vjp: shared memory opt-in");
-    smem_set = true;
-  }
+  const int st = vjp_smem_opt_in<T>();
+  if (st) return st;
   vjp_prim_kernel<T><<<tgrid, tblock, kPrimTiles * tile_bytes, s>>>(a);
   note_launch();
   const int ft = 128;
@@ -1070,9 +1296,9 @@ int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
     const long long nseg = (n + 1 + a.seg - 1) / a.seg;
     const long long threads = (long long)n1 * n2 * nseg;
     const unsigned blocks = (unsigned)((threads + ft - 1) / ft);
-    if (D == 0) vjp_face_kernel<T, 0><<<blocks, ft, 0, s>>>(a);
-    else if (D == 1) vjp_face_kernel<T, 1><<<blocks, ft, 0, s>>>(a);
-    else vjp_face_kernel<T, 2><<<blocks, ft, 0, s>>>(a);
+    if (D == 0) vjp_face_kernel<T, 0, SCHEME, RIEMANN><<<blocks, ft, 0, s>>>(a);
+    else if (D == 1) vjp_face_kernel<T, 1, SCHEME, RIEMANN><<<blocks, ft, 0, s>>>(a);
+    else vjp_face_kernel<T, 2, SCHEME, RIEMANN><<<blocks, ft, 0, s>>>(a);
     note_launch();
   }
   vjp_cell_kernel<T><<<tgrid, tblock, kCellTiles * tile_bytes, s>>>(a);
@@ -1119,10 +1345,13 @@ extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
     return record_error(SWC_ERR_ARG, "stage vjp: NULL argument");
   if (sc->dtype != SWC_F32 && sc->dtype != SWC_F64)
     return record_error(SWC_ERR_ARG, "bad dtype %d", sc->dtype);
-  if (sc->interp != SWC_WENO5 || sc->riemann != SWC_HLLC || sc->nscalars != 0)
+  if ((sc->interp != SWC_WENO5 && sc->interp != SWC_MUSCL) ||
+      (sc->riemann != SWC_HLL && sc->riemann != SWC_HLLC) || sc->nscalars != 0)
     return record_error(SWC_ERR_UNSUPPORTED,
-                        "the stage adjoint covers WENO5 + HLLC without "
-                        "transported scalars");
+                        "the stage adjoint covers WENO5 or MUSCL with HLL or "
+                        "HLLC, without transported scalars");
+  if (sc->interp == SWC_MUSCL && (sc->limiter < 0 || sc->limiter > 3))
+    return record_error(SWC_ERR_ARG, "bad MUSCL limiter %d", sc->limiter);
   if (grid->halo < 3)
     return record_error(SWC_ERR_ARG, "halo_width %d is too small (needs 3)",
                         grid->halo);
@@ -1184,7 +1413,18 @@ extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
   a.gravity_mask = sc->gravity_mask;
   a.nu_bar = nu_bar;
   a.seg = 16;
+  a.limiter = sc->limiter;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  return sc->dtype == SWC_F32 ? launch_vjp<float>(a, bcs, s)
-                              : launch_vjp<double>(a, bcs, s);
+  const bool f32 = sc->dtype == SWC_F32;
+  const bool muscl = sc->interp == SWC_MUSCL, hllc = sc->riemann == SWC_HLLC;
+  if (f32) {
+    if (muscl) return hllc ? launch_vjp<float, 2, 1>(a, bcs, s)
+                           : launch_vjp<float, 2, 0>(a, bcs, s);
+    return hllc ? launch_vjp<float, 0, 1>(a, bcs, s)
+                : launch_vjp<float, 0, 0>(a, bcs, s);
+  }
+  if (muscl) return hllc ? launch_vjp<double, 2, 1>(a, bcs, s)
+                         : launch_vjp<double, 2, 0>(a, bcs, s);
+  return hllc ? launch_vjp<double, 0, 1>(a, bcs, s)
+              : launch_vjp<double, 0, 0>(a, bcs, s);
 }

@@ -1,6 +1,7 @@
 """GPU: the discrete adjoint of whole runs (swc_rk_stage_vjp through
 swirlc_b200.adjoint) against float64 central differences of the same runs,
-h = 1e-6 along seeded random directions in (initial state, nu); plus the
+h = 1e-6 (1e-8 for MUSCL) along seeded random directions in (initial
+state, nu), for WENO5 and MUSCL (each limiter) with HLLC and HLL; plus the
 autograd front end.
 
 The scheme is only piecewise differentiable: HLLC sets s_m to 0 where
@@ -55,7 +56,7 @@ def _loss_grad(s, fields, loss=_loss):
 
 
 def _check_fd(user_cfg, state, steps, k, dts, ndir, seed=0, tol=1e-6,
-              with_nu=True, linear=False):
+              with_nu=True, linear=False, h=1e-6):
   from swirlc_b200 import adjoint
   cfg, s, f = _setup(user_cfg, state)
   loss = _loss
@@ -78,7 +79,6 @@ def _check_fd(user_cfg, state, steps, k, dts, ndir, seed=0, tol=1e-6,
   hw = s.hw
   inner = (slice(hw, -hw),) * 3
   rng = np.random.default_rng(seed)
-  h = 1e-6
   worst = 0.0
   for _ in range(ndir):
     d = []
@@ -145,6 +145,44 @@ def test_rough_gravity_dirichlet_walls_gradient_matches_fd():
   pe = orc.potential_energy(ocfg, state['rho'].shape, np.float64)
   st = _rough(state, 9, p_scale=1e5, pe=pe)
   _check_fd(cfg, st, 3, 2, [1e-5] * 3, ndir=8, seed=2, linear=True)
+
+
+@pytest.mark.parametrize('interp,riemann,limiter', [
+    ('WENO_5', 'HLL', 'mc'),
+    ('MUSCL', 'HLLC', 'van_leer'),
+    ('MUSCL', 'HLL', 'van_leer'),
+    ('MUSCL', 'HLL', 'mc'),
+    ('MUSCL', 'HLL', 'minmod'),
+    ('MUSCL', 'HLL', 'minmod3'),
+])
+def test_rough_scheme_variants_gradient_matches_fd(interp, riemann, limiter):
+  """HLL and the MUSCL limiters on the rough periodic viscous case. The
+  limiters switch branch where dm / dp crosses 0, 1/3, 1 or 3, and on a
+  rough state many slopes lie near a switch: at h = 1e-6 a direction
+  straddles one now and then (minmod: up to 1.3e-4 measured), at h = 1e-7
+  rarely, at h = 1e-8 never in these directions (all <= 1.2e-7, float64
+  rounding; 1e-9 typical where nothing is straddled). Hence h = 1e-8."""
+  from swirlc_b200 import configs
+  cfg, state = configs.kelvin_helmholtz(n=8, nu=1e-2, dtype=np.float64)
+  cfg = dict(cfg, interpolation_scheme=interp, numeric_flux_scheme=riemann,
+             muscl_limiter=limiter)
+  _check_fd(cfg, _rough(state, 11), 3, 2, [1e-3] * 3, ndir=8, seed=3,
+            h=1e-8)
+
+
+def test_muscl_hll_gravity_walls_gradient_matches_fd():
+  """The buoyant bubble's scheme (MUSCL van Leer + HLL, gravity,
+  Dirichlet / Neumann z walls) on a rough state."""
+  from oracle import swirlc_oracle as orc
+  from swirlc_b200 import configs
+  cfg, state = configs.buoyant_bubble(nx=6, ny=6, nz=10, dtype=np.float64)
+  keys = ('halo_width', 'dx', 'dy', 'dz', 'x', 'y', 'z', 'g',
+          'source_functions')
+  ocfg = orc.make_cfg(**{k: cfg[k] for k in keys if k in cfg})
+  pe = orc.potential_energy(ocfg, state['rho'].shape, np.float64)
+  st = _rough(state, 12, p_scale=1e5, pe=pe)
+  _check_fd(cfg, st, 3, 2, [1e-5] * 3, ndir=8, seed=4, with_nu=False,
+            linear=True, h=1e-8)
 
 
 def test_kh_benchmark_setup_gradient_matches_fd():
@@ -266,7 +304,7 @@ def test_float32_adjoint_agrees_with_float64():
 def test_adjoint_rejects_unsupported_schemes():
   from swirlc_b200 import adjoint, configs
   cfg, state = configs.sod(n=24, ny=4, nz=4, dtype=np.float64)
-  cfg = dict(cfg, interpolation_scheme='MUSCL')
+  cfg = dict(cfg, interpolation_scheme='WENO_3')
   _, s, f = _setup(cfg, state)
   run = adjoint.RunAdjoint(s, checkpoint_every=2)
   o = run.run(f, [1e-3])
