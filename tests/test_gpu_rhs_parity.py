@@ -63,7 +63,16 @@ def test_rhs_matches_oracle_periodic(case, dtype):
       'numeric_flux_scheme', 'include_diffusion', 'transport_parameters',
       'muscl_limiter', 'x', 'y', 'z')})
   want = orc.rhs(state, ocfg)
-  tol = 2e-5 if dtype == torch.float32 else 1e-12
+  # float32: 1e-5 against the float32 oracle (measured <= 3.1e-6 over the
+  # cases), and no further from the float64 oracle than twice the float32
+  # oracle's own distance from it (measured ratio <= 1.05).
+  tol = 1e-5 if dtype == torch.float32 else 1e-12
+  exact = None
+  if dtype == torch.float32:
+    exact = orc.rhs({k: v.astype(np.float64) for k, v in state.items()}, ocfg)
   for k in NAMES:
     err = helpers.rel_l2(got[k], want[k], hw)
     assert err < tol, (k, err)
+    if exact is not None:
+      floor = helpers.rel_l2(want[k], exact[k], hw)
+      assert helpers.rel_l2(got[k], exact[k], hw) <= 2.0 * floor, (k, floor)
