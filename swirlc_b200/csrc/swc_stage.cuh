@@ -9,9 +9,10 @@
 // Work decomposition (2.5-D plane marching). A CTA owns a TY x TX column of
 // cells in the (y, x) plane and marches along z over `zseg` planes. A ring
 // of RING planes of primitives (with an in-plane halo HR) lives in shared
-// memory; each step loads one new plane, computes every y- and x-face of the
-// centre plane into shared memory, computes the z-face above each column in
-// registers (the face below is carried from the previous step), then forms
+// memory; each step computes every y- and x-face of the centre plane into
+// shared memory and the z-face above each column in registers (the face
+// below is carried from the previous step), converts the next plane into a
+// ring slot those faces do not read, and after the step's one barrier forms
 // the divergence and the stage update of the centre plane. Each face flux is
 // computed exactly once per CTA. x and y faces reconstruct both face states
 // from the face's stencil; z faces take them from cell-centred
@@ -73,7 +74,16 @@ struct Geom {
   // first pass of a segment also reconstructs its own plane.
   static constexpr int ZLO = cmax(cmax(cmax(LO - 1, CL), VISC ? 1 : 0), 0);
   static constexpr int ZHI = cmax(cmax(cmax(RI, CR + 1), VISC ? 1 : 0), 1);
-  static constexpr int RING = ZLO + 1 + ZHI;
+  // The next plane is converted while the faces of plane zc are still being
+  // read, into the slot of plane zc-ZLO-SPARE. The faces read plane zc, the
+  // planes from zc+1-CL up (the z reconstruction of cell zc+1) and, viscous,
+  // zc-1 (tangential differences), so that slot is free when ZLO >= 1,
+  // ZLO >= CL and, viscous, ZLO >= 2; otherwise one spare slot is added
+  // (not loaded by the warm-up, so the halo depth the arrays need does not
+  // change).
+  static constexpr int SPARE =
+      (ZLO >= 1 && ZLO >= CL && (!VISC || ZLO >= 2)) ? 0 : 1;
+  static constexpr int RING = ZLO + 1 + ZHI + SPARE;
   // Halo layers the stored arrays need.
   static constexpr int NEED = cmax(HR, cmax(ZLO + 1, ZHI));
 };
@@ -94,12 +104,14 @@ struct Layout {
   static constexpr int PER = (PS + NT - 1) / NT;  // plane cells per thread
   static constexpr int RING_ELEMS = G::RING * NV * PS;
   static constexpr int STAGE_ELEMS = NCS * PS;
+  // x- and y-face fluxes, two buffers each (planes alternate), so that
+  // threads may start the next plane's faces while others still form the
+  // update of this one. The z-face flux stays in the registers of the
+  // thread that computes and uses it.
   static constexpr int FY_ELEMS = NF * TX * (TY + 1);
   static constexpr int FX_ELEMS = NF * (TX + 1) * TY;
-  static constexpr int FZ_ELEMS = NF * TX * TY;
   static constexpr size_t SMEM =
-      sizeof(T) * (size_t)(RING_ELEMS + STAGE_ELEMS + FY_ELEMS + FX_ELEMS +
-                           FZ_ELEMS);
+      sizeof(T) * (size_t)(RING_ELEMS + STAGE_ELEMS + 2 * (FY_ELEMS + FX_ELEMS));
 };
 
 // 4- or 8-byte asynchronous global->shared copy (LDGSTS), cached in L1 so
@@ -139,16 +151,15 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
   using L = Layout<T, SCHEME, VISC, TY, TX, NS, HELP>;
   constexpr int NV = L::NV, NCS = L::NCS, NF = L::NF;
   constexpr int LO = G::LO, NW = G::NW, HR = G::HR, ZLO = G::ZLO,
-                ZHI = G::ZHI, RING = G::RING, CL = G::CL, CW = G::CW,
-                NOFF = G::NOFF;
+                ZHI = G::ZHI, RING = G::RING, SPARE = G::SPARE, CL = G::CL,
+                CW = G::CW, NOFF = G::NOFF;
   constexpr int PW = L::PW, PH = L::PH, PS = L::PS, NT = L::NT, PER = L::PER;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* ring = reinterpret_cast<T*>(smem_raw);
-  T* stg = ring + L::RING_ELEMS;  // [NCS][PS] conserved plane in flight
-  T* fy = stg + L::STAGE_ELEMS;   // [NF][TX][TY+1]
-  T* fx = fy + L::FY_ELEMS;       // [NF][TX+1][TY]
-  T* fz = fx + L::FX_ELEMS;       // [NF][TX][TY]
+  T* stg = ring + L::RING_ELEMS;    // [NCS][PS] conserved plane in flight
+  T* fy0 = stg + L::STAGE_ELEMS;    // [2][NF][TX][TY+1]
+  T* fx0 = fy0 + 2 * L::FY_ELEMS;   // [2][NF][TX+1][TY]
 
   const int tid = threadIdx.x;
   // Cell of this thread. For TY = 16 a warp covers rows w and w + TX/2, whose
@@ -494,8 +505,12 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
   };
 
   const int SL = NV * PS;  // ring slot stride
+  // Flux buffers of the plane in progress, and this thread's z-face flux.
+  T* fx = fx0;
+  T* fy = fy0;
+  T fzr[NF];
   // Face of kind `kind` (0 = x-face at row fxx, 1 = y-face at column fyy,
-  // 2 = z-face above plane zc) into the flux buffers.
+  // 2 = z-face above plane zc) into the flux buffers (z: into fzr).
   auto do_face = [&](int kind, int zc, int fxx, int fyy) {
     int off[NOFF], ta[4], tb[4];
     T pe;
@@ -524,7 +539,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
       pe = pe_at(x0 + fxx + h, y0 + fyy + h, zc + 1 + h);
       face(2, off, oa, ob, ta, tb, pe, bside, pidx, f);
 #pragma unroll
-      for (int v = 0; v < NF; ++v) fz[(v * TX + fxx) * TY + fyy] = f[v];
+      for (int v = 0; v < NF; ++v) fzr[v] = f[v];
     } else {
       const int cs = slot_of(zc) * SL;
       const int dm = (slot_of(zc - 1) - slot_of(zc)) * SL;
@@ -549,16 +564,18 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
     }
   };
 
-  // ---- warm-up: planes zfirst .. z0+ZHI-2 through the staging buffer; the
-  // loop's first pass (zc = z0-1) adds plane z0+ZHI-1 and only computes the
-  // z-face below the segment, so that every face of every segment comes from
-  // the same code (results do not depend on where segments start).
-  for (int i = 0; i < RING - 1; ++i) {
+  // ---- warm-up: planes zfirst .. z0+ZHI-1 through the staging buffer (the
+  // ring of the loop's first pass, zc = z0-1, which only computes the z-face
+  // below the segment, so that every face of every segment comes from the
+  // same code: results do not depend on where segments start); plane
+  // z0+ZHI, converted during that pass, in flight.
+  for (int i = 0; i < RING - SPARE; ++i) {
     issue_plane(zfirst + i);
     cp_async_wait_all();
     convert_plane(zfirst + i, i);
   }
-  issue_plane(z0 + ZHI - 1);  // plane of the loop's first pass, in flight
+  if (z0 < z1) issue_plane(z0 + ZHI);
+  __syncthreads();
   const bool own = (x0 + tx < a.nx) && (y0 + ty < a.ny);
   T flo[NF];
 
@@ -594,16 +611,16 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
   const bool ex_x = own && (x0 + tx + 1 == a.nx) && (tx + 1 < TX);
   const bool ex_y = own && (y0 + ty + 1 == a.ny) && (ty + 1 < TY);
 
+  // One barrier per plane: faces of plane zc (x and y into flux buffer
+  // zc & 1, z into registers), then the conversion of plane zc+ZHI+1 into
+  // a slot no face of plane zc reads, the barrier, and the update of plane
+  // zc, which reads no ring slot. A thread may start the faces of plane
+  // zc+1 while others still update plane zc: they write the other flux
+  // buffer, and buffer zc & 1 is next written after the following barrier.
   for (int zc = z0 - 1; zc < z1; ++zc) {
-    // The plane zc+ZHI (staged during the previous plane) replaces the slot
-    // of plane zc-ZLO-1, last read before the barrier that ended the
-    // previous iteration.
-    cp_async_wait_all();
-    convert_plane(zc + ZHI, slot_of(zc + ZHI));
-    __syncthreads();
-    if (zc + 1 < z1) issue_plane(zc + ZHI + 1);
-
     const bool pre = zc < z0;  // only the z-face below the segment
+    fx = fx0 + ((zc - z0 + 1) & 1) * L::FX_ELEMS;
+    fy = fy0 + ((zc - z0 + 1) & 1) * L::FY_ELEMS;
     if (pre && own) {
       // Upper-face value of cell z0-1: the lower state of the segment's
       // first z face.
@@ -636,11 +653,26 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
       }
       do_face(kind, zc, fxx, fyy);
     }
+    // The cell's density for the gravity source, read while plane zc's
+    // slot is certain to hold it (before the barrier).
+    const T rho_cell =
+        (a.gravity_mask && own && !pre) ? R(slot_of(zc), 0, HR + tx, HR + ty)
+                                        : T(0);
+    // Plane zc+ZHI+1 (staged during the previous plane) replaces the slot
+    // of plane zc-ZLO-SPARE, which no face of plane zc reads. The first
+    // pass also read plane zc-CL (its own cell's reconstruction), which can
+    // be that plane: there the other threads' reads are waited for first.
+    if (zc + 1 < z1) {
+      if (pre) __syncthreads();
+      cp_async_wait_all();
+      convert_plane(zc + ZHI + 1, slot_of(zc + ZHI + 1));
+      if (zc + 2 < z1) issue_plane(zc + ZHI + 2);
+    }
     __syncthreads();
     if (pre) {
       if (own) {
 #pragma unroll
-        for (int v = 0; v < NF; ++v) flo[v] = fz[(v * TX + tx) * TY + ty];
+        for (int v = 0; v < NF; ++v) flo[v] = fzr[v];
       }
       continue;
     }
@@ -660,7 +692,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
       T src[5] = {T(0), T(0), T(0), T(0), T(0)};
       if (a.gravity_mask) {
         // Buoyancy acts on rho, or on rho - rho_ref with helper states.
-        T rho_c = R(slot_of(zc), 0, HR + tx, HR + ty);
+        T rho_c = rho_cell;
         if constexpr (HELP)
           rho_c = rho_c - __ldg(static_cast<const T*>(ext->rho_ref) + o);
 #pragma unroll
@@ -671,7 +703,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a,
       T out[NF];
 #pragma unroll
       for (int v = 0; v < NF; ++v) {
-        const T fhi = fz[(v * TX + tx) * TY + ty];
+        const T fhi = fzr[v];
         T rhs = v < 5 ? src[v] : T(0);
         rhs = rhs - divk((fx[(v * (TX + 1) + tx + 1) * TY + ty] -
                      fx[(v * (TX + 1) + tx) * TY + ty]), dx, rdx);
