@@ -85,6 +85,14 @@ __global__ void halo_periodic_kernel(const HaloArgs a, int total,
   if (t < total) halo_shell_elem<T>(a, t, clamp_x, clamp_y, clamp_z);
 }
 
+// One-pass halo fill composing periodic, Dirichlet and Neumann sides
+// (halo_shell_bc_elem, swc_halo.cuh).
+template <typename T>
+__global__ void halo_shell_kernel(const ShellArgs a, int total) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < total) halo_shell_bc_elem<T>(a, t);
+}
+
 // ---------------------------------------------------------------------------
 // CFL reduction, device clock.
 // ---------------------------------------------------------------------------
@@ -493,6 +501,41 @@ int swc_halo_fill(const SwcGrid* grid, int32_t dtype, int32_t nfields,
       else
         halo_periodic_kernel<double><<<blocks, threads, 0, s>>>(
             a, (int)total, clamp[0], clamp[1], clamp[2]);
+      note_launch();
+      return check_launch("halo_fill");
+    }
+    // Every side periodic, Dirichlet or Neumann, none on a primitive
+    // variable, no periodic dim narrower than the halo: one pass that
+    // composes the three (bit for bit the same values).
+    bool one_pass = !any_prim && total < (1LL << 31);
+    ShellArgs sa;
+    memset(&sa, 0, sizeof(sa));
+    sa.nf = nfields;
+    const int nd[3] = {grid->nx, grid->ny, grid->nz};
+    for (int i = 0; i < nfields && one_pass; ++i) {
+      sa.fld[i].f = fields[i];
+      for (int d = 0; d < 3 && one_pass; ++d) {
+        SwcBC lo = bcs[i].side[d][0], hi = bcs[i].side[d][1];
+        if (lo.kind == SWC_BC_PERIODIC || hi.kind == SWC_BC_PERIODIC) {
+          // A periodic side makes the whole dim periodic (boundary.py:65-68).
+          lo.kind = hi.kind = SWC_BC_PERIODIC;
+          if (nd[d] < h) one_pass = false;
+        } else if (lo.kind == SWC_BC_NONE || hi.kind == SWC_BC_NONE) {
+          one_pass = false;
+        }
+        sa.fld[i].bc[d][0] = lo;
+        sa.fld[i].bc[d][1] = hi;
+      }
+    }
+    if (one_pass) {
+      sa.nx = grid->nx; sa.ny = grid->ny; sa.nz = grid->nz; sa.h = h;
+      sa.sx = grid->sx; sa.sz = grid->sz;
+      const int threads = 256;
+      const unsigned blocks = (unsigned)((total + threads - 1) / threads);
+      if (dtype == SWC_F32)
+        halo_shell_kernel<float><<<blocks, threads, 0, s>>>(sa, (int)total);
+      else
+        halo_shell_kernel<double><<<blocks, threads, 0, s>>>(sa, (int)total);
       note_launch();
       return check_launch("halo_fill");
     }

@@ -183,15 +183,12 @@ __device__ __forceinline__ void halo_elem(const A& a, long long t) {
 //
 // Element t of the halo shell (t < halo_shell_count) of the grid in `a`
 // (HaloArgs or HaloMember).
-template <typename T, typename A>
-__device__ __forceinline__ void halo_shell_elem(const A& a, int t, int clamp_x,
-                                                int clamp_y, int clamp_z) {
-  constexpr int NFMAX = sizeof(A::fld) / sizeof(A::fld[0]);
-  const int h = a.h, nx = a.nx, ny = a.ny, nz = a.nz;
+// Padded coordinates (xa, ya, za) of element t of the halo shell.
+__device__ __forceinline__ void shell_cell(int h, int nx, int ny, int nz,
+                                           int t, int& xa, int& ya, int& za) {
   const int nxa = nx + 2 * h, nya = ny + 2 * h;
   const int plane = nxa * nya;
   const int frame = 2 * h * nya + nx * 2 * h;
-  int xa, ya, za;
   if (t < 2 * h * plane) {
     const int zi = t / plane, r = t - zi * plane;
     za = zi < h ? zi : nz + zi;
@@ -213,6 +210,15 @@ __device__ __forceinline__ void halo_shell_elem(const A& a, int t, int clamp_x,
       ya = j < h ? j : ny + j;
     }
   }
+}
+
+template <typename T, typename A>
+__device__ __forceinline__ void halo_shell_elem(const A& a, int t, int clamp_x,
+                                                int clamp_y, int clamp_z) {
+  constexpr int NFMAX = sizeof(A::fld) / sizeof(A::fld[0]);
+  const int h = a.h, nx = a.nx, ny = a.ny, nz = a.nz;
+  int xa, ya, za;
+  shell_cell(h, nx, ny, nz, t, xa, ya, za);
   auto src = [h](int c, int n, int clamp) {
     if (clamp) return c < h ? h : (c >= n + h ? n + h - 1 : c);
     return c < h ? c + n : (c >= n + h ? c - n : c);
@@ -228,6 +234,97 @@ __device__ __forceinline__ void halo_shell_elem(const A& a, int t, int clamp_x,
 #pragma unroll
   for (int f = 0; f < NFMAX; ++f)
     if (f < a.nf) static_cast<T*>(a.fld[f].f)[o] = v[f];
+}
+
+// One-pass fill of fields whose every side is periodic, Dirichlet (a value
+// or per-layer planes) or Neumann (an increment per layer), none of them
+// given on a primitive variable, with no periodic dim narrower than the
+// halo. The x, y, z passes of halo_kernel compose to this: a halo cell's
+// value is made by the last pass whose dim has the cell in its halo.
+// Walking the passes backwards from that one, a periodic dim moves the cell
+// to the cell it wraps to, a Neumann dim moves it to its edge cell (that
+// layer's increments are applied later), and a Dirichlet dim ends the walk
+// with its layer's value at the cell's position; otherwise the walk ends at
+// an interior cell. The value is then rebuilt forwards with the Neumann
+// increments in pass order, one layer at a time as the passes add them, so
+// the result is bit for bit that of the three passes.
+struct ShellField {
+  void* f;
+  SwcBC bc[3][2];  // [x, y, z][low, high]; a periodic dim is so on both sides
+};
+struct ShellArgs {
+  int nf;
+  ShellField fld[SWC_MAX_FIELDS];
+  int nx, ny, nz, h;
+  long long sx, sz;
+};
+
+template <typename T>
+__device__ __forceinline__ void halo_shell_bc_elem(const ShellArgs& a, int t) {
+  const int h = a.h;
+  const int n[3] = {a.nx, a.ny, a.nz};
+  const int ext[3] = {a.nx + 2 * h, a.ny + 2 * h, a.nz + 2 * h};
+  int c0[3];
+  shell_cell(h, a.nx, a.ny, a.nz, t, c0[0], c0[1], c0[2]);
+  // Every load before any store (the compiler cannot tell the fields
+  // apart); the loads are of interior cells and planes, which no thread
+  // writes.
+  T v[SWC_MAX_FIELDS];
+#pragma unroll
+  for (int fi = 0; fi < SWC_MAX_FIELDS; ++fi) {
+    if (fi >= a.nf) break;
+    const ShellField& F = a.fld[fi];
+    int c[3] = {c0[0], c0[1], c0[2]};
+    // Neumann steps met on the way back: layers and side per dim.
+    int nl[3] = {0, 0, 0}, ns[3] = {0, 0, 0};
+    bool dir = false;
+    T val = T(0);
+#pragma unroll
+    for (int d = 2; d >= 0; --d) {
+      const int side = c[d] < h ? 0 : (c[d] >= n[d] + h ? 1 : -1);
+      if (side < 0) continue;
+      const SwcBC& b = side == 0 ? F.bc[d][0] : F.bc[d][1];
+      if (b.kind == SWC_BC_PERIODIC) {
+        c[d] = side == 0 ? c[d] + n[d] : c[d] - n[d];
+      } else if (b.kind == SWC_BC_NEUMANN) {
+        // Layer l lies l + 1 cells from the edge cell.
+        ns[d] = side;
+        nl[d] = side == 0 ? h - c[d] : c[d] - (n[d] + h) + 1;
+        c[d] = side == 0 ? h : n[d] + h - 1;
+      } else {
+        // Dirichlet: layer 0 is the outermost on the low side, the
+        // innermost on the high side; planes are [halo][A][B] with (A, B)
+        // the other two dims in storage order (z, x, y).
+        const int l = side == 0 ? c[d] : c[d] - n[d] - h;
+        if (b.per_layer) {
+          int ia, ib, na, nb;
+          if (d == 0) { ia = c[2]; ib = c[1]; na = ext[2]; nb = ext[1]; }
+          else if (d == 1) { ia = c[2]; ib = c[0]; na = ext[2]; nb = ext[0]; }
+          else { ia = c[0]; ib = c[1]; na = ext[0]; nb = ext[1]; }
+          val = static_cast<const T*>(b.planes)[(long long)l * na * nb +
+                                                (long long)ia * nb + ib];
+        } else {
+          val = T(b.value);
+        }
+        dir = true;
+        break;
+      }
+    }
+    if (!dir)
+      val = static_cast<const T*>(F.f)[c[2] * a.sz + c[0] * a.sx + c[1]];
+    // Forwards: the Neumann steps in pass order x, y, z (only dims after a
+    // Dirichlet one were walked, so only those have steps).
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const T inc = T(ns[d] == 0 ? F.bc[d][0].value : F.bc[d][1].value);
+      for (int l = 0; l < nl[d]; ++l) val = ns[d] == 0 ? val - inc : val + inc;
+    }
+    v[fi] = val;
+  }
+  const long long o = c0[2] * a.sz + c0[0] * a.sx + c0[1];
+#pragma unroll
+  for (int fi = 0; fi < SWC_MAX_FIELDS; ++fi)
+    if (fi < a.nf) static_cast<T*>(a.fld[fi].f)[o] = v[fi];
 }
 
 // Cells of the halo shell of an (nx, ny, nz) grid with halo h.
