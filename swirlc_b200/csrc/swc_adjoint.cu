@@ -1338,6 +1338,7 @@ extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
                                 const void* const* x2, double c2,
                                 void* const* vout, double* nu_bar,
                                 void* const* scratch, void* stream) {
+  swc::NvtxRange nvtx_range_("swc_rk_stage_vjp");
   using namespace swc;
   int st = check_grid(grid);
   if (st) return st;

@@ -407,6 +407,7 @@ int batch_clock(const std::vector<Plan>& plans, int end, cudaStream_t s) {
 extern "C" int swc_batch_step(const SwcScheme* sc, int32_t order,
                               int32_t nmembers, const SwcBatchMember* members,
                               void* stream) {
+  swc::NvtxRange nvtx_range_("swc_batch_step");
   using namespace swc;
   if (!sc) return record_error(SWC_ERR_ARG, "scheme is NULL");
   if (sc->dtype != SWC_F32 && sc->dtype != SWC_F64)

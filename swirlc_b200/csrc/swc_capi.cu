@@ -438,6 +438,7 @@ int64_t swc_launch_count(void) { return g_launches; }
 int swc_halo_fill(const SwcGrid* grid, int32_t dtype, int32_t nfields,
                   void* const* fields, const SwcFieldBC* bcs,
                   int32_t rho_index, void* stream) {
+  swc::NvtxRange nvtx_range_("swc_halo_fill");
   int st = check_grid(grid);
   if (st) return st;
   if (!dtype_ok(dtype)) return fail(SWC_ERR_ARG, "bad dtype %d", dtype);
@@ -686,6 +687,7 @@ int swc_rk_stage(const SwcGrid* grid, const SwcScheme* sc,
                  const void* const* uk, const void* const* u0,
                  void* const* uout, int32_t mode, double c0, double c1,
                  const double* dt, double* dtmin_out, void* stream) {
+  swc::NvtxRange nvtx_range_("swc_rk_stage");
   if (sc && sc->nscalars != 0)
     return fail(SWC_ERR_UNSUPPORTED,
                 "transported scalars go through swc_rk_stage_ext");
@@ -726,6 +728,7 @@ int swc_rk_stage_ext(const SwcGrid* grid, const SwcScheme* sc,
                      const void* const* u0, void* const* uout, int32_t mode,
                      double c0, double c1, const double* dt,
                      double* dtmin_out, void* stream) {
+  swc::NvtxRange nvtx_range_("swc_rk_stage_ext");
   if (!sc) return fail(SWC_ERR_ARG, "scheme is NULL");
   const int ns = sc->nscalars;
   if (ns < 0 || ns > 3)
@@ -798,6 +801,7 @@ int swc_rk_stage_ext(const SwcGrid* grid, const SwcScheme* sc,
 
 int swc_cfl_reduce(const SwcGrid* grid, const SwcScheme* sc,
                    const void* const* u, double* dtmin_out, void* stream) {
+  swc::NvtxRange nvtx_range_("swc_cfl_reduce");
   int st = check_grid(grid);
   if (st) return st;
   if (!sc || !dtype_ok(sc->dtype)) return fail(SWC_ERR_ARG, "bad scheme/dtype");
@@ -1073,6 +1077,7 @@ int swc_rk_combine(int64_t n, int32_t dtype, int32_t mode, double c0,
 int swc_rk_step(const SwcGrid* grid, const SwcScheme* scheme,
                 const SwcFieldBC* bcs, int32_t order, void* const* u,
                 void* const* work, SwcClock* clock_dev, void* stream) {
+  swc::NvtxRange nvtx_range_("swc_rk_step");
   int st = check_grid(grid);
   if (st) return st;
   if (!scheme || !bcs || !u || !work || !clock_dev)

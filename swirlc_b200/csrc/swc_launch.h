@@ -3,10 +3,22 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "swc_stage.cuh"
 
 namespace swc {
+
+// A named NVTX range over one C-ABI call, so that profilers show the
+// library's steps, stages, halo fills and adjoint stages on the host
+// timeline (NVTX v3 is header-only; with no tool attached a push and pop
+// cost a few nanoseconds).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Launches the fused stage kernel for one (dtype, scheme); returns 0 or a
 // negative SWC status. Defined in swc_stage_inst.cu, compiled once per pair.

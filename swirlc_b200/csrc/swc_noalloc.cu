@@ -70,6 +70,7 @@ extern "C" int swc_rk_step_noalloc(const SwcGrid* grid, const SwcScheme* scheme,
                                    const SwcFieldBC* bcs, int32_t order,
                                    void* const* u, SwcClock* clock_dev,
                                    void* stream) {
+  swc::NvtxRange nvtx_range_("swc_rk_step_noalloc");
   if (!grid || !scheme)
     return swc::record_error(SWC_ERR_ARG, "rk_step_noalloc: NULL argument");
   if (scheme->dtype != SWC_F32 && scheme->dtype != SWC_F64)
