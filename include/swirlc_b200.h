@@ -270,12 +270,16 @@ int swc_batch_step(const SwcScheme* scheme, int32_t order, int32_t nmembers,
  * cotangent B*lam + B*dt*H^T J^T lam (alpha = B, beta = B*dt) and the u0
  * cotangent A*lam, which x1 / x2 let the caller fold in. vout must not alias
  * uk, lam, x1 or x2. `scratch` is SWC_VJP_SCRATCH caller buffers of the
- * shape of uk (primitives and their cotangents, and copies transposed to
- * [z][y][x] for the y faces). The first call in a process sets the
- * kernels' shared-memory limit for its dtype: make it outside stream
- * capture. The reference differentiates this path with TF's GradientTape;
- * this is its discrete adjoint. */
-#define SWC_VJP_SCRATCH 33
+ * shape of uk, each holding at least (nx+2h)(ny+2h)(nz+2h) elements and
+ * 8-byte aligned (primitives and their cotangents, copies transposed to
+ * [z][y][x] for the y faces, the per-segment and tangential parts that
+ * are summed in a fixed order, the per-warp nu partials). Every sum has a
+ * fixed order (no floating-point atomics whose order depends on
+ * scheduling), so the same inputs give the same bits on every run. The
+ * first call in a process sets the kernels' shared-memory limit for its
+ * dtype: make it outside stream capture. The reference differentiates
+ * this path with TF's GradientTape; this is its discrete adjoint. */
+#define SWC_VJP_SCRATCH 79
 int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* scheme,
                      const SwcFieldBC* bcs, const void* const* uk,
                      const void* const* lam, double alpha, double beta,

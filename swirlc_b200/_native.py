@@ -86,7 +86,7 @@ class SwcClock(ctypes.Structure):
 
 SWC_MAX_OVERRIDES = 8
 # Scratch buffers of swc_rk_stage_vjp (SWC_VJP_SCRATCH).
-SWC_VJP_SCRATCH = 33
+SWC_VJP_SCRATCH = 79
 SWC_FACE_PRIMITIVE, SWC_FACE_CONSERVATIVE = 0, 1
 SWC_FLUX_CONVECTIVE, SWC_FLUX_DIFFUSIVE, SWC_FLUX_TOTAL = 0, 1, 2
 

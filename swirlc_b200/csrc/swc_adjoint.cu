@@ -17,6 +17,8 @@
 // cell (the reverse of cons_to_prim), then the halo fill is reversed dim by
 // dim in the order z, y, x.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <stdint.h>
 #include <string.h>
 
@@ -633,6 +635,17 @@ struct VjpArgs {
   double alpha, c1, c2;
   const void* x1[5];
   const void* x2[5];
+  // Per face pass D (in that pass's layout), so that every sum has a fixed
+  // order: primitive cotangents of the five cells at the head of each
+  // segment (hb), the cotangents of each cell's four tangential differences
+  // (tg; tgh: the head cell's part from its segment's first face), and the
+  // nu cotangent of every block (nu_part, pass D from nu_off[D]).
+  // vjp_fix_kernel adds the first two to the primitive cotangents.
+  void* hb[3][7];
+  void* tg[3][4];
+  void* tgh[3][4];
+  double* nu_part;
+  long long nu_off[3];
 };
 
 template <typename T>
@@ -648,6 +661,10 @@ __device__ __forceinline__ T pe_of(const VjpArgs& a, int xa, int ya, int za) {
 // cells of one z plane, 4 per thread; the transposed copies go through a
 // shared-memory tile so that both layouts are read and written coalesced.
 constexpr int TT = 32;
+// Faces per thread of a face pass. The five head cells of consecutive
+// segments must not overlap (vjp_fix_kernel adds each once).
+constexpr int kVjpSeg = 16;
+static_assert(kVjpSeg >= 5, "segment heads would overlap");
 
 // Primitives of every cell (halos included), in both layouts, with their
 // cotangent buffers cleared, and lam transposed.
@@ -808,15 +825,23 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
 #pragma unroll
     for (int v = 0; v < 5; ++v) lv[v] = static_cast<const T*>(LAM[v])[o];
   };
+  // A thread flushes cells i0-3 .. i1+1 of its line, each once. The five
+  // head cells i0-3 .. i0+1 are also flushed by the previous segment's
+  // thread (they are its tail): this thread's part goes to hb, which the
+  // fix-up kernel adds. Every other cell gets exactly one addition in this
+  // pass, so the atomic below adds to a value no other thread changes
+  // meanwhile and the sum is the same on every run.
   auto flush = [&](int j, const V2* b, T bh) {
     const long long o = base + (long long)(j + h) * st;
-    atomicAdd(static_cast<T*>(PBAR[0]) + o, b[0].x);
-    atomicAdd(static_cast<T*>(PBAR[vel[0]]) + o, b[1].x);
-    atomicAdd(static_cast<T*>(PBAR[vel[1]]) + o, b[1].y);
-    atomicAdd(static_cast<T*>(PBAR[vel[2]]) + o, b[2].x);
-    atomicAdd(static_cast<T*>(PBAR[4]) + o, b[0].y);
-    atomicAdd(static_cast<T*>(PBAR[5]) + o, b[2].y);
-    atomicAdd(static_cast<T*>(PBAR[6]) + o, bh);
+    const T val[7] = {b[0].x, b[1].x, b[1].y, b[2].x, b[0].y, b[2].y, bh};
+    const int var[7] = {0, vel[0], vel[1], vel[2], 4, 5, 6};
+    if (j <= i0 + 1) {
+#pragma unroll
+      for (int k = 0; k < 7; ++k) static_cast<T*>(a.hb[D][var[k]])[o] = val[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 7; ++k) atomicAdd(static_cast<T*>(PBAR[var[k]]) + o, val[k]);
+    }
   };
   // Window at face i (between cells i-1 and i): primitives sw[k] of cells
   // i-3+k (k = 0..5) and cotangents ab[k] of cells i-3+k (k = 0..4). Step i
@@ -856,27 +881,22 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
   const T scale = T(a.beta) / hd;
   const T nu = T(a.nu), inv_pr = T(1.0 / a.pr);
   const T i2t1 = T(1) / (T(2) * h1), i2t2 = T(1) / (T(2) * h2);
-  T* PB1 = static_cast<T*>(PBAR[vel[1]]);
-  T* PB0 = static_cast<T*>(PBAR[vel[0]]);
-  T* PB2 = static_cast<T*>(PBAR[vel[2]]);
   // Viscous: tangential central differences of cell o (g11, g10, g22, g20:
   // velocity t1 and the normal velocity along t1, velocity t2 and the normal
-  // velocity along t2), and the reverse onto the four neighbours.
+  // velocity along t2). Their cotangents are stored per cell (tg; the head
+  // cell i0-1 of a segment, whose face i0-1 belongs to the previous
+  // segment, into tgh) and moved onto the four neighbours by the fix-up
+  // kernel, which gathers them per target cell in a fixed order.
   auto tang = [&](long long o, T* g4) {
     g4[0] = (P[vel[1]][o + s1] - P[vel[1]][o - s1]) * i2t1;
     g4[1] = (P[vel[0]][o + s1] - P[vel[0]][o - s1]) * i2t1;
     g4[2] = (P[vel[2]][o + s2] - P[vel[2]][o - s2]) * i2t2;
     g4[3] = (P[vel[0]][o + s2] - P[vel[0]][o - s2]) * i2t2;
   };
-  auto tang_flush = [&](long long o, const T* gb) {
-    atomicAdd(PB1 + o + s1, gb[0] * i2t1);
-    atomicAdd(PB1 + o - s1, -gb[0] * i2t1);
-    atomicAdd(PB0 + o + s1, gb[1] * i2t1);
-    atomicAdd(PB0 + o - s1, -gb[1] * i2t1);
-    atomicAdd(PB2 + o + s2, gb[2] * i2t2);
-    atomicAdd(PB2 + o - s2, -gb[2] * i2t2);
-    atomicAdd(PB0 + o + s2, gb[3] * i2t2);
-    atomicAdd(PB0 + o - s2, -gb[3] * i2t2);
+  auto tang_store = [&](long long o, const T* gb, bool head) {
+    void* const* dst = head ? a.tgh[D] : a.tg[D];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) static_cast<T*>(dst[c])[o] = gb[c];
   };
   // Tangential differences of cell i-1 and their cotangent so far.
   T g4a[4] = {T(0), T(0), T(0), T(0)}, gba[4] = {T(0), T(0), T(0), T(0)};
@@ -976,10 +996,11 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
       ab[3][1].y += ubb[1];
       ab[2][2].x += uab[2];
       ab[3][2].x += ubb[2];
-      // Cell i-1's tangential cotangent is complete (faces i-1 and i).
+      // Cell i-1's tangential cotangent is complete (faces i-1 and i),
+      // except at i = i0 (face i0 only: the head part).
 #pragma unroll
       for (int c = 0; c < 4; ++c) gba[c] += gab[c];
-      tang_flush(ob - st, gba);
+      tang_store(ob - st, gba, i == i0);
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         gba[c] = gbb[c];
@@ -1053,15 +1074,142 @@ __global__ void __launch_bounds__(128, SWC_VJP_FACE_MINB)
     // Cells i1-3 .. i1+1 may still hold contributions.
 #pragma unroll
     for (int k = 0; k < 5; ++k) flush(i1 - 3 + k, ab[k], abh[k]);
-    if (a.visc) tang_flush(base + (long long)(i1 - 1 + h) * st, gba);
+    // Cell i1-1: its face i1-1 part (face i1 is the next segment's).
+    if (a.visc) tang_store(base + (long long)(i1 - 1 + h) * st, gba, false);
   }
   if (a.visc && a.nu_bar) {
+    // One partial per block (a fixed shuffle tree per warp, the warps in
+    // order), summed in a fixed order by vjp_nu_kernel.
+    __shared__ double wsum[32];
     double m = double(nub);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
       m += __shfl_xor_sync(0xffffffffu, m, off);
-    if ((threadIdx.x & 31) == 0 && m != 0.0) atomicAdd(a.nu_bar, m);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double b = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += wsum[w];
+      a.nu_part[a.nu_off[D] + blockIdx.x] = b;
+    }
   }
+}
+
+// The parts of face pass D that the pass leaves outside pbar / pbarT, for
+// the target cell (c1, c2, j) of that pass's frame (interior indices; o its
+// offset in the pass's layout), added to acc (7 primitive cotangents): the
+// head parts of the segments (hb) and, viscous, the tangential-difference
+// cotangents of the four neighbouring source cells (tg, plus tgh where the
+// source is the head cell i0-1 of a segment), always in the same order.
+// vjp_fix_kernel calls it once per pass for each cell, so no two threads
+// write one sum and the result does not depend on scheduling.
+template <typename T, int D>
+__device__ __forceinline__ int pass_parts(const VjpArgs& a, int c1, int c2,
+                                          int j, long long o, T* acc) {
+  const int n = D == 0 ? a.nx : (D == 1 ? a.ny : a.nz);
+  const int n1 = D == 0 ? a.ny : a.nx;
+  const int n2 = D == 2 ? a.ny : a.nz;
+  const long long s1 = D == 2 ? a.sx : 1;
+  const long long s2 = D == 0 ? a.sz : (D == 1 ? a.tsz : 1);
+  constexpr int seg = kVjpSeg;  // a.seg
+  const int nseg = (n + 1 + seg - 1) / seg;
+  const bool in1 = c1 >= 0 && c1 < n1, in2 = c2 >= 0 && c2 < n2;
+  const int vel[3] = {1 + D, D == 0 ? 2 : 1, D == 2 ? 2 : 3};
+  int mask = 0;
+  // Head cells of segment sg: sg*seg-3 .. sg*seg+1 (seg >= 5: disjoint).
+  if (in1 && in2 && j >= -3 && (j + 3) % seg <= 4 && (j + 3) / seg < nseg) {
+#pragma unroll
+    for (int v = 0; v < 7; ++v) acc[v] += static_cast<const T*>(a.hb[D][v])[o];
+    mask = 0x7f;
+  }
+  if (!a.visc || j < -1 || j > n || !(in1 || in2) || c1 < -1 || c1 > n1 ||
+      c2 < -1 || c2 > n2)
+    return mask;
+  // Cotangent k of the tangential differences of source cell
+  // (j, c1+d1, c2+d2): its tg value (cells 0 .. n of a line) plus its tgh
+  // value where it is the head cell i0-1 of a segment.
+  const bool hj = (j + 1) % seg == 0 && (j + 1) / seg < nseg;
+  auto src = [&](int k, int d1, int d2) -> T {
+    const int e1 = c1 + d1, e2 = c2 + d2;
+    if (e1 < 0 || e1 >= n1 || e2 < 0 || e2 >= n2) return T(0);
+    const long long q = o + d1 * s1 + d2 * s2;
+    T v = j >= 0 ? static_cast<const T*>(a.tg[D][k])[q] : T(0);
+    if (hj) v += static_cast<const T*>(a.tgh[D][k])[q];
+    return v;
+  };
+  const T h1 = T(D == 0 ? a.dy : a.dx);
+  const T h2 = T(D == 2 ? a.dy : a.dz);
+  const T i2t1 = T(1) / (T(2) * h1), i2t2 = T(1) / (T(2) * h2);
+  // A source adds +g/(2 h_t) to its upper and -g/(2 h_t) to its lower
+  // neighbour along t.
+  acc[vel[1]] += (src(0, -1, 0) - src(0, 1, 0)) * i2t1;
+  acc[vel[0]] += (src(1, -1, 0) - src(1, 1, 0)) * i2t1 +
+                 (src(3, 0, -1) - src(3, 0, 1)) * i2t2;
+  acc[vel[2]] += (src(2, 0, -1) - src(2, 0, 1)) * i2t2;
+  return mask | (1 << vel[0]) | (1 << vel[1]) | (1 << vel[2]);
+}
+
+// The face passes' parts outside pbar / pbarT (pass_parts), one thread per
+// cell of the padded grid: L = 0 adds the x and z passes' parts to pbar
+// (reference layout), L = 1 the y pass's to pbarT (transposed layout). No
+// two threads write one cell.
+template <typename T, int L>
+__global__ void __launch_bounds__(256) vjp_fix_kernel(const VjpArgs a) {
+  const int h = a.h;
+  const unsigned nxa = a.nx + 2 * h, nya = a.ny + 2 * h, nza = a.nz + 2 * h;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nxa * nya * nza) return;
+  // 32-bit division: the host keeps the padded grid below 2^32 cells.
+  const unsigned tt = (unsigned)t;
+  T acc[7] = {T(0), T(0), T(0), T(0), T(0), T(0), T(0)};
+  int mask;
+  long long o;
+  void* const* PB;
+  if (L == 0) {  // (y fastest, x, z)
+    const unsigned q = tt / nya;
+    const int ya = (int)(tt - q * nya);
+    const int za = (int)(q / nxa);
+    const int xa = (int)(q - (unsigned)za * nxa);
+    o = za * a.sz + xa * a.sx + ya;
+    mask = pass_parts<T, 0>(a, ya - h, za - h, xa - h, o, acc);
+    mask |= pass_parts<T, 2>(a, xa - h, ya - h, za - h, o, acc);
+    PB = a.pbar;
+  } else {  // transposed: (x fastest, y, z)
+    const unsigned q = tt / nxa;
+    const int xt = (int)(tt - q * nxa);
+    const int za = (int)(q / nya);
+    const int yt = (int)(q - (unsigned)za * nya);
+    o = za * a.tsz + yt * a.tsy + xt;
+    mask = pass_parts<T, 1>(a, xt - h, za - h, yt - h, o, acc);
+    PB = a.pbarT;
+  }
+  if (!mask) return;
+  // Every load before any store (the compiler cannot tell PB from the
+  // arrays read above, and a load after a store would wait for it).
+  T cur[7];
+#pragma unroll
+  for (int v = 0; v < 7; ++v)
+    cur[v] = (mask >> v) & 1 ? static_cast<const T*>(PB[v])[o] : T(0);
+#pragma unroll
+  for (int v = 0; v < 7; ++v)
+    if ((mask >> v) & 1) static_cast<T*>(PB[v])[o] = cur[v] + acc[v];
+}
+
+// nu_bar += the per-warp partials of the three face passes, summed in a
+// fixed order by one block.
+__global__ void __launch_bounds__(256) vjp_nu_kernel(const double* part,
+                                                     long long count,
+                                                     double* nu_bar) {
+  __shared__ double red[256];
+  double m = 0.0;
+  for (long long i = threadIdx.x; i < count; i += 256) m += part[i];
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *nu_bar += red[0];
 }
 
 // Conserved cotangents of every cell from its primitive cotangents (the
@@ -1181,15 +1329,15 @@ __global__ void __launch_bounds__(256) vjp_cell_kernel(const VjpArgs a) {
   }
 }
 
-// Reverse of the halo fill (swc_halo_fill: x, then y, then z) on vout. The
-// fill is a product of per-dim maps: a halo cell ends up holding the value
-// of the cell (src_x(x), src_y(y), src_z(z)), src_d the identity inside the
-// grid, the wrapped cell (periodic) or the edge cell (Neumann) in the
-// halo, provided every halo dim of the cell is a copy; a Dirichlet (or
-// unfilled) halo dim makes it a value with no source. So each halo cell's
-// cotangent is added to its source cell at once, and cleared. One thread per
-// cell of the padded box (interior threads return at once); several halo
-// cells can share a source (atomics).
+// Reverse of the halo fill (swc_halo_fill: x, then y, then z) on vout.
+// Each forward pass writes the halo layers of one dim over the whole padded
+// plane of the other two, so the fill is H = H_z H_y H_x and its reverse
+// applies H_z^T, H_y^T, H_x^T in turn: one launch per dim, one thread per
+// (field, column along that dim). A thread reads its column's halo cells,
+// clears them and adds each cotangent to the cell it was copied from (the
+// wrapped cell, periodic; the edge cell, Neumann; none, Dirichlet or
+// unfilled). Each column belongs to one thread and its additions come in a
+// fixed order, so the sums do not depend on scheduling.
 struct VjpHalo {
   int nx, ny, nz, h;
   long long sx, sz;
@@ -1198,64 +1346,94 @@ struct VjpHalo {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(256) vjp_halo_kernel(const VjpHalo a) {
+__global__ void __launch_bounds__(256) vjp_halo_kernel(const VjpHalo a,
+                                                       const int d) {
   const int h = a.h;
+  // Plane axes (a, b) of the column's dim d: (x, y) for z, (z, x) for y,
+  // (z, y) for x, the contiguous axis y fastest where it is in the plane.
   const int nxa = a.nx + 2 * h, nya = a.ny + 2 * h, nza = a.nz + 2 * h;
+  const int na = d == 2 ? nxa : nza;
+  const int nb = d == 1 ? nxa : nya;
+  const long long sa = d == 2 ? a.sx : a.sz;
+  const long long sb = d == 1 ? a.sx : 1;
+  const long long sd = d == 0 ? a.sx : (d == 1 ? 1 : a.sz);
+  const int n = d == 0 ? a.nx : (d == 1 ? a.ny : a.nz);
+  const unsigned plane = (unsigned)na * (unsigned)nb;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long cells = (long long)nxa * nya * nza;
-  if (t >= cells) return;
-  int ya, xa, za;
-  if (cells < (1LL << 32)) {  // 32-bit division where the grid fits
-    const unsigned tt = (unsigned)t;
-    const unsigned r = tt / (unsigned)nya;
-    ya = (int)(tt - r * (unsigned)nya);
-    za = (int)(r / (unsigned)nxa);
-    xa = (int)(r - (unsigned)za * (unsigned)nxa);
-  } else {
-    ya = (int)(t % nya);
-    const long long r = t / nya;
-    xa = (int)(r % nxa);
-    za = (int)(r / nxa);
-  }
-  const int c[3] = {xa, ya, za};
-  const int n[3] = {a.nx, a.ny, a.nz};
-  int side[3];
-  bool halo = false;
+  if (t >= 5LL * plane) return;
+  const unsigned tt = (unsigned)t;
+  const int v = (int)(tt / plane);
+  const unsigned pp = tt - (unsigned)v * plane;
+  const int ia = (int)(pp / (unsigned)nb);
+  const int ib = (int)(pp - (unsigned)ia * (unsigned)nb);
+  T* f = static_cast<T*>(a.f[v]) + ia * sa + ib * sb;
+  const int kl = a.kind[v][d][0], kh = a.kind[v][d][1];
+  const bool per = kl == SWC_BC_PERIODIC;  // then kh is too
+  if (h <= 8 && (!per || n >= 2 * h)) {
+    // Every value is read before any is written (the compiler cannot tell
+    // the cells apart, and a load after a store would wait for it). With
+    // n >= 2h the wrapped sources [n, n+h) and [h, 2h) are distinct.
+    T lo[8], hi[8], slo[8], shi[8];
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    side[d] = c[d] < h ? 0 : (c[d] >= n[d] + h ? 1 : -1);
-    halo |= side[d] >= 0;
-  }
-  if (!halo) return;
-  const long long o = za * a.sz + xa * a.sx + ya;
-  // All loads first: the stores below go to arrays the compiler cannot
-  // tell apart from the loaded ones.
-  T val[5];
-#pragma unroll
-  for (int v = 0; v < 5; ++v) val[v] = static_cast<const T*>(a.f[v])[o];
-#pragma unroll
-  for (int v = 0; v < 5; ++v) {
-    T* f = static_cast<T*>(a.f[v]);
-    f[o] = T(0);
-    int src[3];
-    bool copy = true;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      src[d] = c[d];
-      if (side[d] < 0) continue;
-      const int kind = a.kind[v][d][side[d]];
-      if (kind == SWC_BC_PERIODIC)
-        src[d] = side[d] == 0 ? c[d] + n[d] : c[d] - n[d];
-      else if (kind == SWC_BC_NEUMANN)
-        src[d] = side[d] == 0 ? h : n[d] + h - 1;
-      else
-        copy = false;
+    for (int k = 0; k < 8; ++k) {
+      if (k >= h) break;
+      lo[k] = f[k * sd];
+      hi[k] = f[(n + h + k) * sd];
+      if (per) {
+        slo[k] = f[(n + k) * sd];   // source of low halo cell k
+        shi[k] = f[(h + k) * sd];   // source of high halo cell k
+      }
     }
-    // Sources are interior cells (periodic dims have n >= h, checked by
-    // the caller).
-    if (copy && val[v] != T(0))
-      atomicAdd(f + (long long)src[2] * a.sz + (long long)src[0] * a.sx + src[1],
-                val[v]);
+    T elo = T(0), ehi = T(0);
+    if (kl == SWC_BC_NEUMANN || kh == SWC_BC_NEUMANN) {
+      elo = f[h * sd];
+      ehi = f[(n + h - 1) * sd];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (k >= h) break;
+      f[k * sd] = T(0);
+      f[(n + h + k) * sd] = T(0);
+    }
+    if (per) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (k >= h) break;
+        f[(n + k) * sd] = slo[k] + lo[k];
+        f[(h + k) * sd] = shi[k] + hi[k];
+      }
+      return;
+    }
+    // Neumann sides: every halo layer of the side is a copy of its edge
+    // cell (n = 1 makes both edge cells one cell: added in turn).
+    T sl = T(0), sh = T(0);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (k >= h) break;
+      sl += lo[k];
+      sh += hi[k];
+    }
+    if (kl == SWC_BC_NEUMANN && kh == SWC_BC_NEUMANN && n == 1) {
+      f[h * sd] = (elo + sl) + sh;
+    } else {
+      if (kl == SWC_BC_NEUMANN) f[h * sd] = elo + sl;
+      if (kh == SWC_BC_NEUMANN) f[(n + h - 1) * sd] = ehi + sh;
+    }
+    return;
+  }
+  // General widths, or a periodic dim shorter than 2h (wrapped sources
+  // shared by both sides): one cell at a time, in the same order.
+  for (int k = 0; k < h; ++k) {
+    const T lv = f[k * sd], hv = f[(n + h + k) * sd];
+    f[k * sd] = T(0);
+    f[(n + h + k) * sd] = T(0);
+    if (per) {
+      f[(n + k) * sd] += lv;
+      f[(h + k) * sd] += hv;
+    } else {
+      if (kl == SWC_BC_NEUMANN) f[h * sd] += lv;
+      if (kh == SWC_BC_NEUMANN) f[(n + h - 1) * sd] += hv;
+    }
   }
 }
 
@@ -1288,20 +1466,40 @@ int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
   if (st) return st;
   vjp_prim_kernel<T><<<tgrid, tblock, kPrimTiles * tile_bytes, s>>>(a);
   note_launch();
+  // Face passes; the blocks' nu partials of pass D start at nu_off[D].
   const int ft = 128;
+  VjpArgs b = a;
+  unsigned blocks[3];
+  long long parts = 0;
   for (int D = 0; D < 3; ++D) {
     const int n = D == 0 ? a.nx : (D == 1 ? a.ny : a.nz);
     const int n1 = D == 0 ? a.ny : a.nx;
     const int n2 = D == 2 ? a.ny : a.nz;
     const long long nseg = (n + 1 + a.seg - 1) / a.seg;
     const long long threads = (long long)n1 * n2 * nseg;
-    const unsigned blocks = (unsigned)((threads + ft - 1) / ft);
-    if (D == 0) vjp_face_kernel<T, 0, SCHEME, RIEMANN><<<blocks, ft, 0, s>>>(a);
-    else if (D == 1) vjp_face_kernel<T, 1, SCHEME, RIEMANN><<<blocks, ft, 0, s>>>(a);
-    else vjp_face_kernel<T, 2, SCHEME, RIEMANN><<<blocks, ft, 0, s>>>(a);
+    blocks[D] = (unsigned)((threads + ft - 1) / ft);
+    b.nu_off[D] = parts;
+    parts += blocks[D];
+  }
+  for (int D = 0; D < 3; ++D) {
+    if (D == 0) vjp_face_kernel<T, 0, SCHEME, RIEMANN><<<blocks[D], ft, 0, s>>>(b);
+    else if (D == 1) vjp_face_kernel<T, 1, SCHEME, RIEMANN><<<blocks[D], ft, 0, s>>>(b);
+    else vjp_face_kernel<T, 2, SCHEME, RIEMANN><<<blocks[D], ft, 0, s>>>(b);
     note_launch();
   }
-  vjp_cell_kernel<T><<<tgrid, tblock, kCellTiles * tile_bytes, s>>>(a);
+  {
+    const long long cells = (long long)nxa * nya * nza;
+    const unsigned fb = (unsigned)((cells + 255) / 256);
+    vjp_fix_kernel<T, 0><<<fb, 256, 0, s>>>(b);
+    note_launch();
+    vjp_fix_kernel<T, 1><<<fb, 256, 0, s>>>(b);
+    note_launch();
+  }
+  if (b.visc && b.nu_bar) {
+    vjp_nu_kernel<<<1, 256, 0, s>>>(b.nu_part, parts, b.nu_bar);
+    note_launch();
+  }
+  vjp_cell_kernel<T><<<tgrid, tblock, kCellTiles * tile_bytes, s>>>(b);
   note_launch();
   {
     VjpHalo hh;
@@ -1318,9 +1516,14 @@ int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
         hh.kind[v][d][1] = hi;
       }
     }
-    const long long cells = (long long)nxa * nya * nza;
-    vjp_halo_kernel<T><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>(hh);
-    note_launch();
+    // z, then y, then x: the reverse of the fill's order.
+    for (int d = 2; d >= 0; --d) {
+      const long long cols = 5LL * (d == 0 ? (long long)nya * nza
+                                           : (d == 1 ? (long long)nxa * nza
+                                                     : (long long)nxa * nya));
+      vjp_halo_kernel<T><<<(unsigned)((cols + 255) / 256), 256, 0, s>>>(hh, d);
+      note_launch();
+    }
   }
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? SWC_OK
@@ -1400,8 +1603,39 @@ extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
     a.pbarT[k] = scratch[21 + k];
   }
   for (int v = 0; v < 5; ++v) a.lamT[v] = scratch[28 + v];
+  for (int D = 0; D < 3; ++D) {
+    for (int k = 0; k < 7; ++k) a.hb[D][k] = scratch[33 + 7 * D + k];
+    for (int k = 0; k < 4; ++k) {
+      a.tg[D][k] = scratch[54 + 4 * D + k];
+      a.tgh[D][k] = scratch[66 + 4 * D + k];
+    }
+  }
+  a.nu_part = static_cast<double*>(scratch[78]);
   a.tsy = grid->nx + 2 * grid->halo;
   a.tsz = a.tsy * (long long)(grid->ny + 2 * grid->halo);
+  {
+    // The per-block nu partials (doubles) live in scratch field 78.
+    const long long elems = a.tsz * (long long)(grid->nz + 2 * grid->halo);
+    const size_t tsize = sc->dtype == SWC_F32 ? 4 : 8;
+    long long parts = 0, most = 0;
+    const int nd[3] = {grid->nx, grid->ny, grid->nz};
+    for (int D = 0; D < 3; ++D) {
+      const long long n1 = nd[D == 0 ? 1 : 0], n2 = nd[D == 2 ? 1 : 2];
+      const long long threads = n1 * n2 * ((nd[D] + 1 + kVjpSeg - 1) / kVjpSeg);
+      parts += (threads + 127) / 128;
+      // Columns of the halo reverse and cells of the fix-up (32-bit index
+      // arithmetic).
+      most = std::max(most, a.tsz * (long long)(grid->nz + 2 * grid->halo));
+      most = std::max(most, 5LL * (n1 + 2LL * grid->halo) *
+                                (n2 + 2LL * grid->halo));
+    }
+    if ((reinterpret_cast<uintptr_t>(scratch[78]) & 7) != 0 ||
+        parts * 8 > elems * (long long)tsize)
+      return record_error(SWC_ERR_ARG, "stage vjp: scratch field 78 is "
+                          "misaligned or too small");
+    if (most >= (1LL << 32))
+      return record_error(SWC_ERR_ARG, "stage vjp: grid too large");
+  }
   for (int d = 0; d < 3; ++d) {
     a.pe[d] = sc->pe_axis[d];
     if (sc->pe_axis[d]) a.has_pe = 1;
@@ -1413,7 +1647,7 @@ extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
   a.beta = beta;
   a.gravity_mask = sc->gravity_mask;
   a.nu_bar = nu_bar;
-  a.seg = 16;
+  a.seg = kVjpSeg;
   a.limiter = sc->limiter;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const bool f32 = sc->dtype == SWC_F32;
