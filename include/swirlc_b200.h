@@ -287,6 +287,22 @@ int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* scheme,
                      double c2, void* const* vout, double* nu_bar,
                      void* const* scratch, void* stream);
 
+/* Reverse of one whole time step, SSP-RK3 (order 3, rk3.py:87-120) or RK2
+ * (order 2, rk2.py:69-86), in one call: the two or three stage adjoints of
+ * swc_rk_stage_vjp with the step's coefficients. `stages` holds order x 5
+ * pointers, the halo-filled stage states (u, u1[, u2]) the forward step
+ * advanced; g is the cotangent of the step's output, gn receives that of
+ * its input (interior; halos 0), nu_bar (may be NULL) accumulates the nu
+ * cotangent. `work` is 10 caller fields of the grid's shape (the stage
+ * cotangents g1, g2). gn must not alias g, work or a stage. Replaces the
+ * per-step loop a caller of the reference would run under GradientTape
+ * (no counterpart call in the reference). */
+int swc_rk_step_vjp(const SwcGrid* grid, const SwcScheme* scheme,
+                    const SwcFieldBC* bcs, int32_t order,
+                    const void* const* stages, double dt, const void* const* g,
+                    void* const* gn, void* const* work, double* nu_bar,
+                    void* const* scratch, void* stream);
+
 /* dtmin_out <- min(dtmin_out, min over interior cells and dims of
  * delta_d / (|u_d| + c)), c = sqrt(gamma p / rho) (CFL rule of the
  * reference's prototype, demo/swirl_c_prototype.ipynb `solve`). */

@@ -44,6 +44,7 @@ EXPORTED = (
     'swc_rk_step',
     'swc_rk_step_noalloc', 'swc_batch_step', 'swc_rk_stage_ext',
     'swc_rk_stage_vjp',
+    'swc_rk_step_vjp',
 )
 
 # Built-in work space of swc_rk_step_noalloc (SWC_NOALLOC_MAX_BYTES).
@@ -173,6 +174,10 @@ def load(require_cuda: bool = True) -> ctypes.CDLL:
                                        ctypes.POINTER(SwcScheme),
                                        ctypes.POINTER(SwcFieldBC), pp, pp, dbl,
                                        dbl, pp, dbl, pp, dbl, pp, vp, pp, vp]
+      lib.swc_rk_step_vjp.argtypes = [ctypes.POINTER(SwcGrid),
+                                      ctypes.POINTER(SwcScheme),
+                                      ctypes.POINTER(SwcFieldBC), i32, pp, dbl,
+                                      pp, pp, pp, vp, pp, vp]
       lib.swc_batch_step.argtypes = [ctypes.POINTER(SwcScheme), i32, i32,
                                      ctypes.POINTER(SwcBatchMember), vp]
       lib.swc_rk_step_noalloc.argtypes = [ctypes.POINTER(SwcGrid),

@@ -93,15 +93,15 @@ class RunAdjoint:
     while len(self._ckpt_pool) < n:
       self._ckpt_pool.append(self.s.new_fields(zero=False))
 
-  def _step(self, u, dt, buf=None):
-    """One step in place on u with fixed dt; the halo-filled stage states
+  def _step(self, u, i, buf=None):
+    """Step i in place on u with its fixed dt; the halo-filled stage states
     (u, u1, u2) are left in `buf` (scratch buffers when None)."""
     s = self.s
     if buf is None:
       if self._tmp is None:
         self._tmp = self._new_buffers()
       buf = self._tmp
-    dtt = s.dt_tensor(dt)
+    dtt = self._dt_dev[i:i + 1]
     s.fill_halos(u)
     u0, w1 = buf[0], buf[1]
     for a, b in zip(u0, u):
@@ -123,6 +123,10 @@ class RunAdjoint:
     self.s.check_fields(fields)
     self.generation += 1
     self.dts = [float(d) for d in dts]
+    # Every step's dt on the device in one copy: a copy per step from
+    # pageable host memory would wait for the stream each time.
+    self._dt_dev = torch.tensor(self.dts or [0.0], dtype=torch.float64,
+                                device=self.s.device)
     u = [f.detach().clone() for f in fields]
     self.checkpoints = []
     self._kept = -1
@@ -133,9 +137,9 @@ class RunAdjoint:
     # The final segment's stage states stay in the pool: the reverse sweep
     # starts there, so it needs no recompute of that segment.
     last_seg = (len(self.dts) - 1) // self.k if self.k and self.dts else -1
-    for i, dt in enumerate(self.dts):
+    for i in range(len(self.dts)):
       if self.k == 0:
-        self._step(u, dt, self._pool[i])
+        self._step(u, i, self._pool[i])
         continue
       if i % self.k == 0:
         c = i // self.k
@@ -144,9 +148,9 @@ class RunAdjoint:
           a.copy_(b)
         self.checkpoints.append(self._ckpt_pool[c])
       if i // self.k == last_seg:
-        self._step(u, dt, self._pool[i - last_seg * self.k])
+        self._step(u, i, self._pool[i - last_seg * self.k])
       else:
-        self._step(u, dt)
+        self._step(u, i)
     self._kept = last_seg
     if self.k == 0:
       self.checkpoints = [None]
@@ -168,7 +172,18 @@ class RunAdjoint:
 
   def _reverse_step(self, stages, dt, g, gn, g2, g1) -> None:
     """gn = cotangent of the step's input for the cotangent g of its
-    output."""
+    output: one swc_rk_step_vjp call (its two or three stage adjoints are
+    the `_vjp` calls of `_reverse_step_by_stage`)."""
+    s = self.s
+    flat = [f for st in stages[:self.order] for f in st]
+    nat.check(nat.load().swc_rk_step_vjp(
+        ctypes.byref(s.grid), ctypes.byref(s.scheme), s.bcs, self.order,
+        nat.ptr_array(flat), float(dt), nat.ptr_array(g), nat.ptr_array(gn),
+        nat.ptr_array(list(g1) + list(g2)), self._nu_bar.data_ptr(),
+        nat.ptr_array(self._scratch), nat.stream_ptr()), 'step vjp')
+
+  def _reverse_step_by_stage(self, stages, dt, g, gn, g2, g1) -> None:
+    """The same reverse step as three (RK2: two) stage adjoints."""
     if self.order == 3:
       u0, u1, u2 = stages
       self._vjp(u2, g, 2.0 / 3.0, 2.0 / 3.0 * dt, g2)
@@ -209,7 +224,7 @@ class RunAdjoint:
           for a, b in zip(u, self.checkpoints[c]):
             a.copy_(b)
           for i in range(first, last):
-            self._step(u, self.dts[i], self._pool[i - first])
+            self._step(u, i, self._pool[i - first])
         # The pool now holds segment c; later sweeps recompute everything.
         self._kept = -1
         for i in reversed(range(first, last)):

@@ -1534,6 +1534,16 @@ int launch_vjp(const VjpArgs& a, const SwcFieldBC* bcs, cudaStream_t s) {
 }  // namespace
 }  // namespace swc
 
+namespace swc {
+namespace {
+int stage_vjp(const SwcGrid* grid, const SwcScheme* sc, const SwcFieldBC* bcs,
+              const void* const* uk, const void* const* lam, double alpha,
+              double beta, const void* const* x1, double c1,
+              const void* const* x2, double c2, void* const* vout,
+              double* nu_bar, void* const* scratch, void* stream);
+}  // namespace
+}  // namespace swc
+
 extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
                                 const SwcFieldBC* bcs, const void* const* uk,
                                 const void* const* lam, double alpha,
@@ -1542,7 +1552,65 @@ extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
                                 void* const* vout, double* nu_bar,
                                 void* const* scratch, void* stream) {
   swc::NvtxRange nvtx_range_("swc_rk_stage_vjp");
+  return swc::stage_vjp(grid, sc, bcs, uk, lam, alpha, beta, x1, c1, x2, c2,
+                        vout, nu_bar, scratch, stream);
+}
+
+// The reversed step: for u' = SSP-RK3(u) (rk3.py:87-120) with stages
+//   u1 = u + dt L(u), u2 = 3/4 u + 1/4 (u1 + dt L(u1)),
+//   u' = 1/3 u + 2/3 (u2 + dt L(u2)),
+// a cotangent g of u' gives g2 = 2/3 g + V(u2, g, 2/3 dt),
+// g1 = 1/4 g2 + V(u1, g2, 1/4 dt), gn = 1/3 g + 3/4 g2 + g1 + V(u, g1, dt);
+// for RK2 (rk2.py:69-86, u' = 1/2 u + 1/2 (u1 + dt L(u1))):
+// g1 = 1/2 g + V(u1, g, 1/2 dt), gn = 1/2 g + g1 + V(u, g1, dt).
+extern "C" int swc_rk_step_vjp(const SwcGrid* grid, const SwcScheme* sc,
+                               const SwcFieldBC* bcs, int32_t order,
+                               const void* const* stages, double dt,
+                               const void* const* g, void* const* gn,
+                               void* const* work, double* nu_bar,
+                               void* const* scratch, void* stream) {
+  swc::NvtxRange nvtx_range_("swc_rk_step_vjp");
   using namespace swc;
+  if (order != 2 && order != 3)
+    return record_error(SWC_ERR_UNSUPPORTED,
+                        "Runge-Kutta order %d is not implemented", order);
+  if (!stages || !g || !gn || !work)
+    return record_error(SWC_ERR_ARG, "step vjp: NULL argument");
+  const void* const* u0 = stages;
+  const void* const* u1 = stages + 5;
+  void* const* w1 = work;      // g1
+  void* const* w2 = work + 5;  // g2 (RK3)
+  for (int v = 0; v < 5; ++v)
+    for (int k = 0; k < 5 * order; ++k)
+      if (gn[v] == stages[k])
+        return record_error(SWC_ERR_ARG, "step vjp: gn must not alias a stage");
+  int rc;
+  if (order == 3) {
+    const void* const* u2 = stages + 10;
+    if ((rc = stage_vjp(grid, sc, bcs, u2, g, 2.0 / 3.0, 2.0 / 3.0 * dt,
+                        nullptr, 0.0, nullptr, 0.0, w2, nu_bar, scratch,
+                        stream)))
+      return rc;
+    if ((rc = stage_vjp(grid, sc, bcs, u1, w2, 0.25, 0.25 * dt, nullptr, 0.0,
+                        nullptr, 0.0, w1, nu_bar, scratch, stream)))
+      return rc;
+    return stage_vjp(grid, sc, bcs, u0, w1, 1.0, dt, g, 1.0 / 3.0, w2, 0.75,
+                     gn, nu_bar, scratch, stream);
+  }
+  if ((rc = stage_vjp(grid, sc, bcs, u1, g, 0.5, 0.5 * dt, nullptr, 0.0,
+                      nullptr, 0.0, w1, nu_bar, scratch, stream)))
+    return rc;
+  return stage_vjp(grid, sc, bcs, u0, w1, 1.0, dt, g, 0.5, nullptr, 0.0, gn,
+                   nu_bar, scratch, stream);
+}
+
+namespace swc {
+namespace {
+int stage_vjp(const SwcGrid* grid, const SwcScheme* sc, const SwcFieldBC* bcs,
+              const void* const* uk, const void* const* lam, double alpha,
+              double beta, const void* const* x1, double c1,
+              const void* const* x2, double c2, void* const* vout,
+              double* nu_bar, void* const* scratch, void* stream) {
   int st = check_grid(grid);
   if (st) return st;
   if (!sc || !bcs || !uk || !lam || !vout || !scratch)
@@ -1663,3 +1731,6 @@ extern "C" int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* sc,
   return hllc ? launch_vjp<double, 0, 1>(a, bcs, s)
               : launch_vjp<double, 0, 0>(a, bcs, s);
 }
+
+}  // namespace
+}  // namespace swc

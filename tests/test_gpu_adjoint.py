@@ -345,3 +345,26 @@ def test_adjoint_rejects_unsupported_schemes():
   o = run.run(f, [1e-3])
   with pytest.raises(NotImplementedError):
     run.backward(_loss_grad(s, o))
+
+
+@pytest.mark.parametrize('scheme', ['rk3', 'rk2'])
+def test_step_vjp_equals_its_stage_vjps(scheme):
+  """swc_rk_step_vjp (one call per reversed step) gives the bits of its two
+  or three swc_rk_stage_vjp calls made one by one."""
+  from swirlc_b200 import adjoint, configs
+  cfg, state = configs.kelvin_helmholtz(n=16, nu=1e-2, dtype=np.float64)
+  _, s, f = _setup(cfg, state, torch.float32)
+  run = adjoint.RunAdjoint(s, checkpoint_every=0, scheme=scheme)
+  run.run(f, [2e-3] * 2)
+  stages = run._pool[1]
+  gen = torch.Generator(device='cuda').manual_seed(5)
+  g = [torch.randn(x.shape, generator=gen, device='cuda') for x in f]
+  outs = []
+  for fn in (run._reverse_step, run._reverse_step_by_stage):
+    run._nu_bar.zero_()
+    gn, g2, g1 = (s.new_fields(zero=True) for _ in range(3))
+    fn(stages, 2e-3, g, gn, g2, g1)
+    outs.append(([x.clone() for x in gn], float(run._nu_bar.item())))
+  for a, b in zip(outs[0][0], outs[1][0]):
+    assert torch.equal(a, b)
+  assert outs[0][1] == outs[1][1] != 0.0
