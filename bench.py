@@ -345,8 +345,9 @@ def run_decomposed(args):
   """One Kelvin-Helmholtz domain of --n^3 cells split into the cx x cy x cz
   blocks of --decomposed (strong scaling): one block per rank over
   torch.distributed (NCCL) when launched with cx*cy*cz ranks, else every
-  block in this process (LocalExchange). Halo updates overlap the inner
-  boxes' stage work (decomposition.DecomposedStepper)."""
+  block in this process (LocalExchange). With NCCL (or --overlap) the halo
+  updates overlap the inner boxes' stage work
+  (decomposition.DecomposedStepper); --no-overlap turns that off."""
   import torch
   import torch.distributed as dist
   from swirlc_b200 import configs, decomposition
@@ -370,7 +371,7 @@ def run_decomposed(args):
   mine = {rank: blocks[rank]} if world > 1 else blocks
   ds = decomposition.DecomposedStepper(
       user_cfg, mine, transport='dist' if world > 1 else 'local',
-      overlap=False if args.no_overlap else True)
+      overlap=False if args.no_overlap else (True if args.overlap else None))
   ds.step(args.warmup)
   torch.cuda.synchronize()
 
@@ -1107,6 +1108,10 @@ def main():
   ap.add_argument('--no-overlap', action='store_true',
                   help='--decomposed: halo update before each stage instead '
                        'of behind the inner boxes')
+  ap.add_argument('--overlap', action='store_true',
+                  help='--decomposed: halo update behind the inner boxes '
+                       'also with all blocks in this process (by default '
+                       'only the NCCL transport overlaps)')
   ap.add_argument('--profile-steps', type=int, default=0,
                   help='only run this many eager RK3 steps of the workload '
                        '(a small, untimed command for ncu captures)')

@@ -874,12 +874,13 @@ def cfl_dt_min(cons, cfg, pe=None):
     pe = potential_energy(cfg, cons[RHO].shape, cons[RHO].dtype)
   prim = conservative_to_primitive(cons)
   p = pressure(prim, pe)
-  c = np.sqrt(GAMMA * p / prim[RHO])
+  # Interior cells only: halo layers may hold values no fill has set.
   sl = (slice(hw, -hw or None),) * 3
+  c = np.sqrt(GAMMA * p[sl] / prim[RHO][sl])
   dts = []
   for d, vel in zip(DIMS, VELOCITY):
     delta = {'x': cfg.dx, 'y': cfg.dy, 'z': cfg.dz}[d]
-    dts.append(np.min(delta / (np.abs(prim[vel][sl]) + c[sl])))
+    dts.append(np.min(delta / (np.abs(prim[vel][sl]) + c)))
   return float(min(dts))
 
 
