@@ -294,7 +294,8 @@ int swc_rk_stage_vjp(const SwcGrid* grid, const SwcScheme* scheme,
  * advanced; g is the cotangent of the step's output, gn receives that of
  * its input (interior; halos 0), nu_bar (may be NULL) accumulates the nu
  * cotangent. `work` is 10 caller fields of the grid's shape (the stage
- * cotangents g1, g2). gn must not alias g, work or a stage. Replaces the
+ * cotangents g1, then g2; RK2 uses only g1). gn must not alias g, work or a
+ * stage (SWC_ERR_ARG, checked before any launch). Replaces the
  * per-step loop a caller of the reference would run under GradientTape
  * (no counterpart call in the reference). */
 int swc_rk_step_vjp(const SwcGrid* grid, const SwcScheme* scheme,

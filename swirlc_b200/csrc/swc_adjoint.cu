@@ -1580,10 +1580,17 @@ extern "C" int swc_rk_step_vjp(const SwcGrid* grid, const SwcScheme* sc,
   const void* const* u1 = stages + 5;
   void* const* w1 = work;      // g1
   void* const* w2 = work + 5;  // g2 (RK3)
-  for (int v = 0; v < 5; ++v)
+  for (int v = 0; v < 5; ++v) {
     for (int k = 0; k < 5 * order; ++k)
       if (gn[v] == stages[k])
         return record_error(SWC_ERR_ARG, "step vjp: gn must not alias a stage");
+    for (int k = 0; k < 5; ++k)
+      if (gn[v] == g[k])
+        return record_error(SWC_ERR_ARG, "step vjp: gn must not alias g");
+    for (int k = 0; k < 5 * (order - 1); ++k)
+      if (gn[v] == work[k])
+        return record_error(SWC_ERR_ARG, "step vjp: gn must not alias work");
+  }
   int rc;
   if (order == 3) {
     const void* const* u2 = stages + 10;

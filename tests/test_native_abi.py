@@ -58,6 +58,27 @@ def test_argument_errors_need_no_gpu(lib):
                                    0.0, None, None, None))
 
 
+def test_step_vjp_argument_errors_need_no_gpu(lib):
+  # Order and aliasing checks run before any CUDA call; the pointers are
+  # only compared, never dereferenced.
+  def arr(lo, hi):
+    return (ctypes.c_void_p * (hi - lo))(*[0x10000 + 256 * i
+                                          for i in range(lo, hi)])
+  stages, g, work = arr(0, 15), arr(15, 20), arr(20, 30)
+  gn, scratch = arr(30, 35), arr(35, 40)
+  with pytest.raises(NotImplementedError):
+    nat.check(lib.swc_rk_step_vjp(None, None, None, 4, stages, 1e-3, g, gn,
+                                  work, None, scratch, None))
+  for bad in (arr(10, 15), arr(15, 20), arr(25, 30)):  # a stage, g, work
+    with pytest.raises(ValueError):
+      nat.check(lib.swc_rk_step_vjp(None, None, None, 3, stages, 1e-3, g, bad,
+                                    work, None, scratch, None))
+  # RK2: gn must not alias g1 (work[0:5]) either.
+  with pytest.raises(ValueError):
+    nat.check(lib.swc_rk_step_vjp(None, None, None, 2, stages, 1e-3, g,
+                                  arr(20, 25), work, None, scratch, None))
+
+
 def test_noalloc_limit_matches_header():
   with open(os.path.join(ROOT, 'include', 'swirlc_b200.h')) as f:
     text = f.read()
