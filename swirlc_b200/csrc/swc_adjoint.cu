@@ -1215,8 +1215,11 @@ __global__ void __launch_bounds__(256) vjp_nu_kernel(const double* part,
 // Conserved cotangents of every cell from its primitive cotangents (the
 // reverse of cons_to_prim), plus the gravity source rho*G*g. The y faces'
 // cotangents are read back from the transposed layout through a tile.
+// Two resident blocks per SM in single precision (128 registers, 8 bytes
+// spilled: 1.7 % off the checkpointed KH 128^3 sweep, same gradient bits);
+// double precision needs ~250 registers and keeps one.
 template <typename T>
-__global__ void __launch_bounds__(256) vjp_cell_kernel(const VjpArgs a) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) vjp_cell_kernel(const VjpArgs a) {
   T(*tiles)[TT][TT + 1] = vjp_tiles<T>();  // as in vjp_prim_kernel
   const int nxa = a.nx + 2 * a.h, nya = a.ny + 2 * a.h;
   const int za = blockIdx.z;
